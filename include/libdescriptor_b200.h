@@ -1,0 +1,212 @@
+/*
+ * libdescriptor_b200.h -- C ABI of the B200 (sm_100a) descriptor library.
+ *
+ * A drop-in for libdescriptor's per-atom descriptor hot path: Behler
+ * symmetry functions and the SNAP-style bispectrum, their forward pass and
+ * the reverse-mode gradient (vector-Jacobian product) w.r.t. coordinates.
+ * All arithmetic is FP64.  Plain pointers and sizes only; every entry point
+ * returns an int status (LD_OK == 0) and sets a thread-local message that
+ * ld_error_message() returns.
+ *
+ * Input layout is the reference's (src/Descriptors.cpp:121-163):
+ *   coords[n_total*3]        contributing atoms first, then ghost images
+ *   species[n_total]         species code 0..n_species-1
+ *   number_of_neighs[rows]   neighbour count of each centre row
+ *   neighbor_list[sum]       neighbour indices (into coords), rows in order
+ *   desc[rows*width]         one row per centre
+ * Batches concatenate configurations: centre of row (c, j) is
+ * j + config_ptr[c]; neighbour indices are global.
+ */
+#ifndef LIBDESCRIPTOR_B200_H_
+#define LIBDESCRIPTOR_B200_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LD_OK 0
+#define LD_ERR_INVALID_KIND 1     /* descriptor kind not supported        */
+#define LD_ERR_INVALID_ARG 2      /* bad size, pointer or index           */
+#define LD_ERR_CAPACITY 3         /* a fixed capacity of the kernels      */
+#define LD_ERR_OOM 4              /* device or host allocation failed     */
+#define LD_ERR_CUDA 5             /* CUDA runtime error                   */
+#define LD_ERR_TIMEOUT 6          /* a bounded device wait ran out        */
+#define LD_ERR_NO_DEVICE 7        /* no CUDA device visible               */
+#define LD_ERR_PARSE 8            /* descriptor parameter file malformed  */
+
+/* Descriptor kinds, numbered as the reference's AvailableDescriptor enum
+ * (include/Descriptors.hpp:21-26). */
+#define LD_KIND_SYMMETRY_FUNCTIONS 0
+#define LD_KIND_BISPECTRUM 1
+#define LD_KIND_SOAP 2
+#define LD_KIND_XI 3
+
+typedef struct ld_descriptor ld_descriptor; /* opaque, owns device tables */
+typedef void *ld_stream;                    /* a cudaStream_t (0 = legacy) */
+
+/* Last error of the calling thread ("" if none). */
+const char *ld_error_message(void);
+/* Library version as 10000*major + 100*minor + patch. */
+int ld_version(void);
+
+/* ---------------- creation (DescriptorKind::initDescriptor) ---------------- */
+
+/* Symmetry functions.  Replaces DescriptorKind::initDescriptor(kind, species,
+ * cutoff_function, cutoff, types, sizes, params) (include/Descriptors.hpp:250-254,
+ * src/Descriptors.cpp:579-590; SymmetryFunctions ctor
+ * src/SymmetryFunctions.cpp:429-451).  type_codes[t] in 1..5 (g1..g5);
+ * sizes[2t], sizes[2t+1] = rows, params per row of block t; params is the
+ * concatenation of the row-major blocks; cutoff_matrix is n_species^2
+ * row-major (the reference's direct init fills it with cutoff[0]). */
+int ld_create_symmetry_functions(ld_descriptor **out, int n_species,
+                                 const double *cutoff_matrix, int n_types,
+                                 const int *type_codes, const int *sizes,
+                                 const double *params);
+
+/* Bispectrum.  Replaces DescriptorKind::initDescriptor(kind, rfac0, twojmax,
+ * diagonalstyle, use_shared_arrays, rmin0, switch_flag, bzero_flag, cutoff,
+ * species, weights) (include/Descriptors.hpp:257-260,
+ * src/Descriptors.cpp:592-607; Bispectrum ctor src/Bispectrum.cpp:44-82).
+ * twojmax <= 10.  use_shared_arrays is accepted and ignored (memory layout
+ * is the library's own). */
+int ld_create_bispectrum(ld_descriptor **out, double rfac0, int twojmax,
+                         int diagonalstyle, int use_shared_arrays, double rmin0,
+                         int switch_flag, int bzero_flag, int n_species,
+                         const double *cutoff_matrix, const double *weights);
+
+/* Parameter-file init.  Replaces DescriptorKind::initDescriptor(file, kind)
+ * (include/Descriptors.hpp:201-202; SymmetryFunctions::initFromFile
+ * src/SymmetryFunctions.cpp:266-407, Bispectrum::initFromFile
+ * src/Bispectrum.cpp:852-1007). */
+int ld_create_from_file(ld_descriptor **out, const char *path, int kind);
+
+int ld_destroy(ld_descriptor *d);
+int ld_width(const ld_descriptor *d, int *width);   /* DescriptorKind::width */
+int ld_kind(const ld_descriptor *d, int *kind);     /* DescriptorKind::descriptor_kind */
+
+/* ---------------- host-pointer API (staging through the device) ----------- */
+
+/* Descriptor::compute (src/Descriptors.cpp:121-136).  desc[n_atoms*width]
+ * is overwritten. */
+int ld_compute(ld_descriptor *d, int n_atoms, int n_total, const int *species,
+               const int *neighbor_list, const int *number_of_neighs,
+               const double *coords, double *desc);
+
+/* Descriptor::gradient (src/Descriptors.cpp:165-260) for the coordinates:
+ * d_coords[n_total*3] = sum_{i,k} dE_ddesc[i,k] d desc[i,k] / d coords
+ * (overwritten, ghost rows unfolded, as the reference returns them).
+ * desc_out (nullable) receives the forward descriptors of the same pass. */
+int ld_gradient(ld_descriptor *d, int n_atoms, int n_total, const int *species,
+                const int *neighbor_list, const int *number_of_neighs,
+                const double *coords, const double *dE_ddesc, double *d_coords,
+                double *desc_out);
+
+/* Descriptor::compute_batch (src/Descriptors.cpp:138-163). */
+int ld_compute_batch(ld_descriptor *d, int n_configs, const int *n_atoms,
+                     const int *config_ptr, int n_total, const int *species,
+                     const int *neighbor_list, const int *number_of_neighs,
+                     const double *coords, double *desc);
+
+/* Descriptor::gradient_batch (src/Descriptors.cpp:263-352). */
+int ld_gradient_batch(ld_descriptor *d, int n_configs, const int *n_atoms,
+                      const int *config_ptr, int n_total, const int *species,
+                      const int *neighbor_list, const int *number_of_neighs,
+                      const double *coords, const double *dE_ddesc,
+                      double *d_coords, double *desc_out);
+
+/* Descriptor::compute_single_atom (src/Descriptors.cpp:355-365):
+ * desc[width] of centre `index` with its own neighbour list. */
+int ld_compute_single_atom(ld_descriptor *d, int index, int n_total,
+                           const int *species, const int *neighbors, int n_neigh,
+                           const double *coords, double *desc);
+
+/* Descriptor::gradient_single_atom (src/Descriptors.cpp:368-452):
+ * d_coords[n_total*3] = dE_ddesc . d desc_index / d coords (overwritten). */
+int ld_gradient_single_atom(ld_descriptor *d, int index, int n_total,
+                            const int *species, const int *neighbors, int n_neigh,
+                            const double *coords, const double *dE_ddesc,
+                            double *d_coords, double *desc_out);
+
+/* Descriptor::jacobian (src/Descriptors.cpp:454-486): J[(width*n_atoms) x
+ * (n_total*3)], row r = d desc_flat[r] / d coords_flat (overwritten). */
+int ld_jacobian(ld_descriptor *d, int n_atoms, int n_total, const int *species,
+                const int *neighbor_list, const int *number_of_neighs,
+                const double *coords, double *J);
+
+/* ---------------- device-pointer API (stream ordered) ---------------------- */
+/* All array arguments are device pointers.  neigh_offsets[n_rows+1] is the
+ * exclusive prefix sum of number_of_neighs (see ld_neighbor_offsets_dev);
+ * row_centre[n_rows] (nullable: centre == row) maps rows to centre atoms.
+ * Nothing is synchronised; errors raised inside kernels are reported by the
+ * next ld_sync_status() on this descriptor. */
+
+/* Exclusive prefix sum of number_of_neighs into neigh_offsets[n_rows+1];
+ * when max_neigh != NULL it also returns max(number_of_neighs) (this
+ * synchronises the stream). */
+int ld_neighbor_offsets_dev(ld_descriptor *d, int n_rows, const int *number_of_neighs,
+                            long long *neigh_offsets, int *max_neigh, ld_stream stream);
+
+/* desc[n_rows*width] overwritten.  max_neigh bounds every row's neighbour
+ * count (it sizes on-chip staging); a row above it raises LD_ERR_CAPACITY
+ * through ld_sync_status and its outputs are set to NaN. */
+int ld_compute_dev(ld_descriptor *d, int n_rows, const int *row_centre,
+                   const int *species, const int *neighbor_list,
+                   const long long *neigh_offsets, int max_neigh,
+                   const double *coords, double *desc, ld_stream stream);
+
+/* d_coords is ACCUMULATED into (the caller zeroes it), like the reference's
+ * gradient shadow.  image (nullable, device int[n_total]) folds each ghost
+ * row onto its contributing master row image[g] (the reference's
+ * assemble_forces, python_package/libdescriptor/neighbor.py:227-263), in
+ * which case d_coords has n_atoms rows where n_atoms > max(image).
+ * desc_out (nullable) receives the forward descriptors. */
+int ld_gradient_dev(ld_descriptor *d, int n_rows, const int *row_centre,
+                    const int *species, const int *neighbor_list,
+                    const long long *neigh_offsets, int max_neigh,
+                    const double *coords,
+                    const double *dE_ddesc, double *d_coords, double *desc_out,
+                    const int *image, ld_stream stream);
+
+/* Wait for `stream` and return the first device-side error status raised by
+ * this descriptor's kernels since the last call (then clear it). */
+int ld_sync_status(ld_descriptor *d, ld_stream stream);
+
+/* ---------------- neighbour lists (python_bindings/neighbor) -------------- */
+
+/* nbl_create_paddings (python_bindings/neighbor/neighbor_list.cpp:283-418):
+ * ghost images of `coords` within `cutoff` of the periodic cell faces.
+ * Call with pad_* == NULL to get *n_pad, then again with buffers of that
+ * size (pad_coords n_pad*3, pad_species n_pad, pad_image n_pad). */
+int ld_create_paddings(double cutoff, const double *cell, const int *pbc,
+                       const double *coords, const int *species, int n_atoms,
+                       int *n_pad, double *pad_coords, int *pad_species,
+                       int *pad_image);
+
+/* nbl_build (neighbor_list.cpp:78-243) with one cutoff, flattened to the
+ * (number_of_neighs, neighbor_list) layout of the rows 0..n_query-1.  Call
+ * with neighbor_list == NULL to get *nnz (counts are filled), then again. */
+int ld_build_neighbor_list(const double *coords, int n_total, double cutoff,
+                           const int *need_neigh, int n_query,
+                           int *number_of_neighs, int *neighbor_list,
+                           long long *nnz);
+
+/* ---------------- measurement helpers ------------------------------------- */
+
+/* Run `iters` rounds of FP64 fused multiply-adds on the device and report
+ * the achieved FP64 rate (TFLOP/s, FMA = 2 flops).  Used as the roofline
+ * denominator of the FP64-bound kernels. */
+int ld_measure_fp64_peak(int iters, double *tflops);
+
+/* Cost of one FP64 library call in FP64-pipe flops at the rate
+ * fp64_tflops (from ld_measure_fp64_peak): op 0 exp, 1 sincos, 2 sqrt,
+ * 3 divide, 4 tan, 5 pow, 6 cos.  Weights transcendental calls in the
+ * algorithmic flop counts of the roofline. */
+int ld_measure_fp64_op_cost(int op, int iters, double fp64_tflops, double *flop_equiv);
+
+/* Number of this library's kernel launches issued so far (all descriptors). */
+long long ld_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LIBDESCRIPTOR_B200_H_ */

@@ -1,0 +1,1048 @@
+// ld_core.cpp -- host side of the C ABI: descriptor handles, parameter and
+// Clebsch-Gordan tables, the bispectrum work schedule, staging of host
+// buffers, and the device-pointer entry points.
+#include <algorithm>
+#include <array>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <mutex>
+#include <queue>
+#include <set>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "ld_internal.h"
+
+// ======================================================================
+// errors, launch accounting, device buffers
+// ======================================================================
+namespace ldb {
+
+static thread_local std::string g_err;
+static std::atomic<long long> g_launches{0};
+
+void set_error(const std::string &msg) { g_err = msg; }
+int fail(int code, const std::string &msg) {
+    g_err = msg;
+    return code;
+}
+int cuda_fail(cudaError_t e, const char *what) {
+    g_err = std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e);
+    if (e == cudaErrorMemoryAllocation) return LD_ERR_OOM;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return LD_ERR_NO_DEVICE;
+    return LD_ERR_CUDA;
+}
+void count_launch(int n) { g_launches += n; }
+
+int DevBuf::ensure(size_t n) {
+    if (n <= bytes && p) return LD_OK;
+    release();
+    size_t want = n < 256 ? 256 : n;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        bytes = 0;
+        return cuda_fail(e, "cudaMalloc");
+    }
+    bytes = want;
+    return LD_OK;
+}
+void DevBuf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+// Packs host vectors into one device allocation (256-byte aligned slots).
+struct Arena {
+    std::vector<char> host;
+    std::vector<std::pair<size_t, const void **>> fix;  // offset, pointer to patch
+    template <class T> void add(const std::vector<T> &v, const T **dst) {
+        size_t off = (host.size() + 255) & ~(size_t)255;
+        host.resize(off + std::max<size_t>(v.size() * sizeof(T), 1));
+        if (!v.empty()) std::memcpy(host.data() + off, v.data(), v.size() * sizeof(T));
+        fix.emplace_back(off, reinterpret_cast<const void **>(dst));
+    }
+    int upload(DevBuf &buf) {
+        int rc = buf.ensure(host.size());
+        if (rc) return rc;
+        LDB_CUDA(cudaMemcpy(buf.p, host.data(), host.size(), cudaMemcpyHostToDevice));
+        for (auto &f : fix) *f.second = static_cast<const char *>(buf.p) + f.first;
+        return LD_OK;
+    }
+};
+
+// ======================================================================
+// Clebsch-Gordan coefficients (Racah formula), doubled-integer arguments:
+// j1, j2, j are 2*(angular momentum); m1 in 0..j1 indexes 2*m = 2*m1 - j1.
+// Same definition as Bispectrum::init_clebsch_gordan (src/Bispectrum.cpp:
+// 683-727); factorials are exact products in double.
+// ======================================================================
+static double fact(int n) {
+    double f = 1.0;
+    for (int k = 2; k <= n; ++k) f *= (double)k;
+    return f;
+}
+
+static double clebsch_gordan(int j1, int j2, int j, int m1, int m2) {
+    const int a2 = 2 * m1 - j1, b2 = 2 * m2 - j2;   // 2*m of the two inputs
+    const int c2 = a2 + b2;                        // 2*m of the output
+    if (c2 < -j || c2 > j) return 0.0;
+    // physical combinations (all integers by the triangle/parity rules)
+    const int s1 = (j1 + j2 - j) / 2, s2 = (j1 - j2 + j) / 2, s3 = (-j1 + j2 + j) / 2;
+    const int top = (j1 + j2 + j) / 2 + 1;
+    const int p1 = (j1 + a2) / 2, q1 = (j1 - a2) / 2;
+    const int p2 = (j2 + b2) / 2, q2 = (j2 - b2) / 2;
+    const int p3 = (j + c2) / 2, q3 = (j - c2) / 2;
+    const int kmin = std::max(0, std::max((j2 - j - a2) / 2, (j1 - j + b2) / 2));
+    const int kmax = std::min(s1, std::min(q1, p2));
+    double sum = 0.0;
+    for (int k = kmin; k <= kmax; ++k) {
+        const double den = fact(k) * fact(s1 - k) * fact(q1 - k) * fact(p2 - k) *
+                           fact((j - j2 + a2) / 2 + k) * fact((j - j1 - b2) / 2 + k);
+        sum += ((k & 1) ? -1.0 : 1.0) / den;
+    }
+    const double tri = std::sqrt(fact(s1) * fact(s2) * fact(s3) / fact(top));
+    const double mf = std::sqrt(fact(p1) * fact(q1) * fact(p2) * fact(q2) * fact(p3) * fact(q3) *
+                                (double)(j + 1));
+    return sum * tri * mf;
+}
+
+}  // namespace ldb
+
+// ======================================================================
+// descriptor handle
+// ======================================================================
+struct ld_descriptor {
+    int kind = -1;
+    int width = 0;
+    int device = 0;
+    ldb::SFDev sf;
+    ldb::BSDev bs;
+    ldb::DevBuf tables;
+    // host-API staging (grow-only)
+    ldb::DevBuf species, nbl, off, coords, desc, dE, dc, centre, list, status, tmp;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    // introspection
+    std::vector<int> bs_out_j1, bs_out_j2, bs_out_j;
+    long long bs_inner_fwd = 0, bs_inner_vjp = 0;  // CG inner iterations per centre
+    int bs_tasks_fwd = 0, bs_tasks_vjp = 0;
+};
+
+namespace ldb {
+
+static int ensure_stream(ld_descriptor *d) {
+    if (d->stream) return LD_OK;
+    LDB_CUDA(cudaSetDevice(d->device));
+    LDB_CUDA(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking));
+    return LD_OK;
+}
+
+static int check_device() {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0)
+        return fail(LD_ERR_NO_DEVICE, std::string("no CUDA device visible (") +
+                                          (e == cudaSuccess ? "count 0" : cudaGetErrorString(e)) + ")");
+    return LD_OK;
+}
+
+// ------------------------------------------------------ symmetry functions
+static int build_sf(ld_descriptor *d, int ns, const double *cutoff, int n_types,
+                    const int *codes, const int *sizes, const double *params) {
+    if (ns <= 0 || !cutoff) return fail(LD_ERR_INVALID_ARG, "symmetry functions: n_species must be > 0");
+    if (n_types < 0 || (n_types > 0 && (!codes || !sizes)))
+        return fail(LD_ERR_INVALID_ARG, "symmetry functions: bad type list");
+    std::vector<double> rcut(cutoff, cutoff + (size_t)ns * ns);
+    std::vector<int> o2, t2, o3, t3, zi3;
+    std::vector<double> a2, b2, P3, z3, l3, e3;
+    struct Three { int o, t; double zeta, lam, eta; };
+    std::vector<Three> three;
+    int width = 0;
+    size_t poff = 0;
+    for (int b = 0; b < n_types; ++b) {
+        const int t = codes[b], rows = sizes[2 * b], cols = sizes[2 * b + 1];
+        if (t < 1 || t > 5) return fail(LD_ERR_INVALID_ARG, "symmetry functions: type code " + std::to_string(t) + " is not g1..g5");
+        if (rows < 0 || cols < 0) return fail(LD_ERR_INVALID_ARG, "symmetry functions: negative block size");
+        const int need = (t == 1) ? 0 : (t == 2) ? 2 : (t == 3) ? 1 : 3;
+        if (rows > 0 && cols < need)
+            return fail(LD_ERR_INVALID_ARG, "symmetry functions: g" + std::to_string(t) + " needs " +
+                                                std::to_string(need) + " parameters per row");
+        if (rows * cols > 0 && !params) return fail(LD_ERR_INVALID_ARG, "symmetry functions: params is NULL");
+        for (int q = 0; q < rows; ++q) {
+            const double *pp = params ? params + poff + (size_t)q * cols : nullptr;
+            const int o = width + q;
+            if (t <= 3) {
+                o2.push_back(o);
+                t2.push_back(t);
+                a2.push_back(cols > 0 ? pp[0] : 0.0);
+                b2.push_back(cols > 1 ? pp[1] : 0.0);
+            } else {
+                three.push_back({o, t, pp[0], pp[1], pp[2]});
+            }
+        }
+        poff += (size_t)rows * cols;
+        width += rows;
+    }
+    std::stable_sort(three.begin(), three.end(), [](const Three &x, const Three &y) {
+        if (x.t != y.t) return x.t < y.t;
+        return x.eta < y.eta;
+    });
+    for (auto &q : three) {
+        o3.push_back(q.o);
+        t3.push_back(q.t);
+        z3.push_back(q.zeta);
+        l3.push_back(q.lam);
+        e3.push_back(q.eta);
+        P3.push_back(std::pow(2, 1 - q.zeta));
+        const bool integral = q.zeta >= 0 && q.zeta <= 64 && std::floor(q.zeta) == q.zeta;
+        zi3.push_back(integral ? (int)q.zeta : -1);
+    }
+    if ((int)o2.size() > 64 || (int)o3.size() > 64)
+        return fail(LD_ERR_CAPACITY, "symmetry functions: at most 64 outputs of one body order are supported");
+    SFDev &s = d->sf;
+    s.ns = ns;
+    s.width = width;
+    s.n2 = (int)o2.size();
+    s.n3 = (int)o3.size();
+    Arena ar;
+    ar.add(rcut, &s.rcut);
+    ar.add(o2, &s.o2);
+    ar.add(t2, &s.t2);
+    ar.add(a2, &s.a2);
+    ar.add(b2, &s.b2);
+    ar.add(o3, &s.o3);
+    ar.add(t3, &s.t3);
+    ar.add(P3, &s.P3);
+    ar.add(z3, &s.z3);
+    ar.add(l3, &s.l3);
+    ar.add(e3, &s.e3);
+    ar.add(zi3, &s.zi3);
+    int rc = ar.upload(d->tables);
+    if (rc) return rc;
+    d->kind = LD_KIND_SYMMETRY_FUNCTIONS;
+    d->width = width;
+    return LD_OK;
+}
+
+// ------------------------------------------------------------- bispectrum
+// Output triples per diagonal style (src/Bispectrum.cpp:84-193, 429-468).
+static bool bs_outputs(int J, int style, std::vector<std::array<int, 3>> &out) {
+    out.clear();
+    switch (style) {
+    case 0:
+        for (int j1 = 0; j1 <= J; ++j1)
+            for (int j2 = 0; j2 <= j1; ++j2)
+                for (int j = j1 - j2; j <= std::min(J, j1 + j2); j += 2) out.push_back({j1, j2, j});
+        return true;
+    case 1:
+        for (int j1 = 0; j1 <= J; ++j1)
+            for (int j = 0; j <= std::min(J, 2 * j1); j += 2) out.push_back({j1, j1, j});
+        return true;
+    case 2:
+        for (int j1 = 0; j1 <= J; ++j1) out.push_back({j1, j1, j1});
+        return true;
+    case 3:
+        for (int j1 = 0; j1 <= J; ++j1)
+            for (int j2 = 0; j2 <= j1; ++j2)
+                for (int j = j1 - j2; j <= std::min(J, j1 + j2); j += 2)
+                    if (j >= j1) out.push_back({j1, j2, j});
+        return true;
+    }
+    return false;
+}
+
+struct BSTask {
+    int t, ma, mb;
+    long long cost;
+};
+
+// Longest-processing-time assignment of Z-element tasks to kBSThreads
+// threads; tasks of one thread are stored contiguously, costliest first.
+static void lpt_schedule(const std::vector<BSTask> &tasks_in, const std::vector<std::array<int, 4>> &trip,
+                         const std::vector<int> &cgoff, std::vector<int> &toff, std::vector<int4> &packed) {
+    std::vector<BSTask> tasks = tasks_in;
+    std::stable_sort(tasks.begin(), tasks.end(), [](const BSTask &a, const BSTask &b) { return a.cost > b.cost; });
+    const int nt = kBSThreads;
+    std::vector<std::vector<BSTask>> bins(nt);
+    using E = std::pair<long long, int>;
+    std::priority_queue<E, std::vector<E>, std::greater<E>> heap;
+    for (int b = 0; b < nt; ++b) heap.push({0, b});
+    for (auto &tk : tasks) {
+        E e = heap.top();
+        heap.pop();
+        bins[e.second].push_back(tk);
+        e.first += tk.cost;
+        heap.push(e);
+    }
+    toff.assign(nt + 1, 0);
+    packed.clear();
+    for (int b = 0; b < nt; ++b) {
+        toff[b] = (int)packed.size();
+        for (auto &tk : bins[b]) {
+            const auto &tr = trip[tk.t];
+            const int j = tr[2], nc = j / 2 + 1;
+            int4 v;
+            v.x = tr[0] | (tr[1] << 8) | (j << 16) | (tk.ma << 24);
+            v.y = tk.mb;
+            v.z = tr[3] + tk.ma * nc + tk.mb;
+            v.w = cgoff[tk.t];
+            packed.push_back(v);
+        }
+    }
+    toff[nt] = (int)packed.size();
+}
+
+static int build_bs(ld_descriptor *d, double rfac0, int J, int style, double rmin0, int switch_flag,
+                    int bzero_flag, int ns, const double *cutoff, const double *weights) {
+    if (J < 0 || J > kMaxTwoJ)
+        return fail(J < 0 ? LD_ERR_INVALID_ARG : LD_ERR_CAPACITY,
+                    "bispectrum: twojmax=" + std::to_string(J) + " outside 0.." + std::to_string(kMaxTwoJ));
+    if (style < 0 || style > 3)
+        return fail(LD_ERR_INVALID_ARG, "bispectrum: diagonalstyle " + std::to_string(style) + " is not a valid index");
+    if (ns <= 0 || !cutoff || !weights) return fail(LD_ERR_INVALID_ARG, "bispectrum: species/cutoff/weights missing");
+    const int D = J + 1;
+    BSDev &b = d->bs;
+    b.J = J;
+    b.style = style;
+    b.switch_flag = switch_flag;
+    b.bzero_flag = bzero_flag;
+    b.ns = ns;
+    b.rfac0 = rfac0;
+    b.rmin0 = rmin0;
+    b.wself = 1.0;
+    // cutoff of neighbour species js is element [js] of the flattened matrix
+    // (the reference reads rcuts(iSpecies, jSpecies) from an Array2D whose
+    // extents are never set, src/Bispectrum.cpp:271,305)
+    std::vector<double> rcut_flat(cutoff, cutoff + ns);
+    std::vector<double> wj(weights, weights + ns);
+    std::vector<double> bzero(D, 0.0);
+    if (bzero_flag)
+        for (int j = 1; j <= J; ++j) bzero[j] = b.wself * b.wself * b.wself * j;
+    std::vector<double> rootpq((size_t)D * D, 0.0);
+    for (int p = 1; p <= J; ++p)
+        for (int q = 1; q <= J; ++q) rootpq[p * D + q] = std::sqrt((double)p / q);
+    std::vector<int> ublock(J + 2, 0), lblock(J + 2, 0);
+    for (int j = 0; j <= J; ++j) {
+        ublock[j + 1] = ublock[j] + (j + 1) * (j + 1);
+        lblock[j + 1] = lblock[j] + (j + 1) * (j / 2 + 1);
+    }
+    b.nU = ublock[J + 1];
+    b.nL = lblock[J + 1];
+    std::vector<int> lel(b.nL);
+    for (int j = 0; j <= J; ++j)
+        for (int ma = 0; ma <= j; ++ma)
+            for (int mb = 0; mb <= j / 2; ++mb) lel[lblock[j] + ma * (j / 2 + 1) + mb] = j | (ma << 8) | (mb << 16);
+    // all j1 >= j2 triples
+    std::vector<std::array<int, 4>> trip;  // j1, j2, j, zoff
+    std::map<std::array<int, 3>, int> tindex;
+    std::vector<int> cgoff;
+    std::vector<double> cg;
+    int zoff = 0;
+    for (int j1 = 0; j1 <= J; ++j1)
+        for (int j2 = 0; j2 <= j1; ++j2)
+            for (int j = j1 - j2; j <= std::min(J, j1 + j2); j += 2) {
+                tindex[{j1, j2, j}] = (int)trip.size();
+                trip.push_back({j1, j2, j, zoff});
+                zoff += (j + 1) * (j / 2 + 1);
+                cgoff.push_back((int)cg.size());
+                for (int m1 = 0; m1 <= j1; ++m1)
+                    for (int m2 = 0; m2 <= j2; ++m2) cg.push_back(clebsch_gordan(j1, j2, j, m1, m2));
+            }
+    b.ntrip = (int)trip.size();
+    b.nZall = zoff;
+    std::vector<std::array<int, 3>> outs;
+    bs_outputs(J, style, outs);
+    b.ncoeff = (int)outs.size();
+    std::vector<int> otrip;
+    d->bs_out_j1.clear();
+    d->bs_out_j2.clear();
+    d->bs_out_j.clear();
+    for (auto &o : outs) {
+        otrip.push_back(tindex.at(o));
+        d->bs_out_j1.push_back(o[0]);
+        d->bs_out_j2.push_back(o[1]);
+        d->bs_out_j.push_back(o[2]);
+    }
+    // Gradient map.  B(a,b,c) = sum_{all ma,mb} Re(conj(U_c) Z_abc) is, by
+    // the Clebsch-Gordan symmetries, also (a+1)/(c+1) sum Re(conj(U_a) Z_cba)
+    // and (b+1)/(c+1) sum Re(conj(U_b) Z_cab); so dB/dU_x for each of its
+    // three factors is a Z array of another triple, scaled.  betaj_t collects
+    // those scaled dL/dB per triple t (first index ordered >= second, Z being
+    // symmetric in its first two indices) and Y_j = sum_t betaj_t Z_t.
+    std::vector<std::map<int, double>> M(trip.size());
+    auto tri = [&](int x, int y, int z) { return tindex.at({std::max(x, y), std::min(x, y), z}); };
+    for (int o = 0; o < (int)outs.size(); ++o) {
+        const int a = outs[o][0], bb = outs[o][1], c = outs[o][2];
+        M[tri(a, bb, c)][o] += 1.0;
+        M[tri(c, bb, a)][o] += (double)(c + 1) / (a + 1);
+        M[tri(c, a, bb)][o] += (double)(c + 1) / (bb + 1);
+    }
+    std::vector<int> moff(trip.size() + 1, 0), mo;
+    std::vector<double> mcoef;
+    for (size_t t = 0; t < trip.size(); ++t) {
+        moff[t] = (int)mo.size();
+        for (auto &kv : M[t]) {
+            mo.push_back(kv.first);
+            mcoef.push_back(kv.second);
+        }
+    }
+    moff[trip.size()] = (int)mo.size();
+    std::vector<int> jtoff(J + 2, 0), jtlist;
+    for (int j = 0; j <= J; ++j) {
+        jtoff[j] = (int)jtlist.size();
+        for (size_t t = 0; t < trip.size(); ++t)
+            if (trip[t][2] == j && !M[t].empty()) jtlist.push_back((int)t);
+    }
+    jtoff[J + 1] = (int)jtlist.size();
+    // Z-element tasks: (triple, ma, mb<=j/2) except the mirror rows of the
+    // middle column, which neither B nor Y reads.
+    std::set<int> need_f(otrip.begin(), otrip.end()), need_v = need_f;
+    for (size_t t = 0; t < trip.size(); ++t)
+        if (!M[t].empty()) need_v.insert((int)t);
+    auto make_tasks = [&](const std::set<int> &need, long long &inner) {
+        std::vector<BSTask> tasks;
+        inner = 0;
+        for (int t : need) {
+            const int j1 = trip[t][0], j2 = trip[t][1], j = trip[t][2];
+            for (int mb = 0; 2 * mb <= j; ++mb)
+                for (int ma = 0; ma <= j; ++ma) {
+                    if (j % 2 == 0 && mb == j / 2 && ma > j / 2) continue;
+                    const int na = std::min(j1, (2 * ma - j + j2 + j1) / 2) - std::max(0, (2 * ma - j - j2 + j1) / 2) + 1;
+                    const int nb = std::min(j1, (2 * mb - j + j2 + j1) / 2) - std::max(0, (2 * mb - j - j2 + j1) / 2) + 1;
+                    const long long c = (long long)std::max(na, 0) * std::max(nb, 0);
+                    inner += c;
+                    tasks.push_back({t, ma, mb, c + 2});
+                }
+        }
+        return tasks;
+    };
+    std::vector<int> toff_f, toff_v;
+    std::vector<int4> task_f, task_v;
+    {
+        auto tf = make_tasks(need_f, d->bs_inner_fwd);
+        lpt_schedule(tf, trip, cgoff, toff_f, task_f);
+        auto tv = make_tasks(need_v, d->bs_inner_vjp);
+        lpt_schedule(tv, trip, cgoff, toff_v, task_v);
+        d->bs_tasks_fwd = (int)tf.size();
+        d->bs_tasks_vjp = (int)tv.size();
+    }
+    std::vector<int4> trip4;
+    for (auto &t : trip) trip4.push_back(make_int4(t[0], t[1], t[2], t[3]));
+    Arena ar;
+    ar.add(rcut_flat, &b.rcut_flat);
+    ar.add(wj, &b.wj);
+    ar.add(bzero, &b.bzero);
+    ar.add(rootpq, &b.rootpq);
+    ar.add(ublock, &b.ublock);
+    ar.add(lblock, &b.lblock);
+    ar.add(trip4, &b.trip);
+    ar.add(cgoff, &b.cgoff);
+    ar.add(cg, &b.cg);
+    ar.add(otrip, &b.otrip);
+    ar.add(moff, &b.moff);
+    ar.add(mo, &b.mo);
+    ar.add(mcoef, &b.mcoef);
+    ar.add(jtoff, &b.jtoff);
+    ar.add(jtlist, &b.jtlist);
+    ar.add(lel, &b.lel);
+    ar.add(toff_f, &b.toff_f);
+    ar.add(task_f, &b.task_f);
+    ar.add(toff_v, &b.toff_v);
+    ar.add(task_v, &b.task_v);
+    int rc = ar.upload(d->tables);
+    if (rc) return rc;
+    d->kind = LD_KIND_BISPECTRUM;
+    d->width = b.ncoeff;
+    return LD_OK;
+}
+
+// ------------------------------------------------------------ host staging
+struct HostRows {
+    int n_rows = 0;
+    std::vector<int> centre;   // empty: centre == row
+    std::vector<long long> off;
+    int maxn = 0;
+    long long nnz = 0;
+};
+
+static int make_rows(int n_rows, const int *counts, HostRows &h) {
+    h.n_rows = n_rows;
+    h.off.assign((size_t)n_rows + 1, 0);
+    h.maxn = 0;
+    for (int r = 0; r < n_rows; ++r) {
+        if (counts[r] < 0) return fail(LD_ERR_INVALID_ARG, "number_of_neighs[" + std::to_string(r) + "] < 0");
+        h.off[r + 1] = h.off[r] + counts[r];
+        h.maxn = std::max(h.maxn, counts[r]);
+    }
+    h.nnz = h.off[n_rows];
+    return LD_OK;
+}
+
+static int validate(const ld_descriptor *d, const HostRows &h, int n_total, const int *species,
+                    const int *nbl) {
+    const int ns = d->kind == LD_KIND_SYMMETRY_FUNCTIONS ? d->sf.ns : d->bs.ns;
+    for (int a = 0; a < n_total; ++a)
+        if (species[a] < 0 || species[a] >= ns)
+            return fail(LD_ERR_INVALID_ARG, "species[" + std::to_string(a) + "]=" + std::to_string(species[a]) +
+                                                " outside 0.." + std::to_string(ns - 1));
+    for (long long q = 0; q < h.nnz; ++q)
+        if (nbl[q] < 0 || nbl[q] >= n_total)
+            return fail(LD_ERR_INVALID_ARG, "neighbor_list[" + std::to_string(q) + "]=" + std::to_string(nbl[q]) +
+                                                " outside 0.." + std::to_string(n_total - 1));
+    if (!h.centre.empty()) {
+        for (int r = 0; r < h.n_rows; ++r)
+            if (h.centre[r] < 0 || h.centre[r] >= n_total)
+                return fail(LD_ERR_INVALID_ARG, "centre atom " + std::to_string(h.centre[r]) + " outside coords");
+    } else if (h.n_rows > n_total) {
+        return fail(LD_ERR_INVALID_ARG, "n_atoms exceeds the number of coordinates");
+    }
+    return LD_OK;
+}
+
+int launch_rows(ld_descriptor *d, const RowArgs &a, cudaStream_t s) {
+    if (d->kind == LD_KIND_SYMMETRY_FUNCTIONS) return sf_launch(d->sf, a, s);
+    return bs_launch(d->bs, a, s);
+}
+
+static int read_status(ld_descriptor *d, cudaStream_t s) {
+    if (!d->status.p) return LD_OK;
+    int st = 0;
+    LDB_CUDA(cudaMemcpyAsync(&st, d->status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    LDB_CUDA(cudaStreamSynchronize(s));
+    if (st != 0) {
+        LDB_CUDA(cudaMemsetAsync(d->status.p, 0, sizeof(int), s));
+        LDB_CUDA(cudaStreamSynchronize(s));
+        if (st == kDevCapacity) return fail(LD_ERR_CAPACITY, "a centre has more neighbours than max_neigh");
+        return fail(LD_ERR_INVALID_ARG, "a neighbour or centre index lies outside the coordinates");
+    }
+    return LD_OK;
+}
+
+static int ensure_status(ld_descriptor *d) {
+    if (d->status.p) return LD_OK;
+    int rc = d->status.ensure(sizeof(int) * 4);
+    if (rc) return rc;
+    LDB_CUDA(cudaMemset(d->status.p, 0, sizeof(int) * 4));
+    return LD_OK;
+}
+
+// Generic host-buffer pass: stage, launch, copy back.  dE == nullptr means
+// forward only.  dcoords (n_total*3) and desc are overwritten when given.
+// jac_width > 0 turns rows into (centre, component) pairs of a Jacobian.
+static int host_pass(ld_descriptor *d, HostRows &h, int n_total, const int *species, const int *nbl,
+                     const double *coords, const double *dE, double *dcoords, double *desc,
+                     int jac_width = 0) {
+    if (!d) return fail(LD_ERR_INVALID_ARG, "descriptor handle is NULL");
+    if (h.n_rows < 0 || n_total < 0) return fail(LD_ERR_INVALID_ARG, "negative size");
+    if (h.n_rows > 0 && (!species || !coords || (h.nnz > 0 && !nbl)))
+        return fail(LD_ERR_INVALID_ARG, "NULL input array");
+    if (dE && h.n_rows > 0 && !dcoords) return fail(LD_ERR_INVALID_ARG, "d_coords is NULL");
+    if (!dE && h.n_rows > 0 && !desc) return fail(LD_ERR_INVALID_ARG, "desc is NULL");
+    int rc = validate(d, h, n_total, species, nbl);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(d->mu);
+    if ((rc = ensure_stream(d)) || (rc = ensure_status(d))) return rc;
+    cudaStream_t s = d->stream;
+    const int W = d->width;
+    const int rows = jac_width > 0 ? h.n_rows * jac_width : h.n_rows;
+    if (rows == 0 && !dE) return LD_OK;
+    if ((rc = d->species.ensure(sizeof(int) * std::max(n_total, 1))) || (rc = d->nbl.ensure(sizeof(int) * std::max<long long>(h.nnz, 1))) ||
+        (rc = d->off.ensure(sizeof(long long) * (h.n_rows + 1))) || (rc = d->coords.ensure(sizeof(double) * 3 * std::max(n_total, 1))))
+        return rc;
+    LDB_CUDA(cudaMemcpyAsync(d->species.p, species, sizeof(int) * n_total, cudaMemcpyHostToDevice, s));
+    if (h.nnz) LDB_CUDA(cudaMemcpyAsync(d->nbl.p, nbl, sizeof(int) * h.nnz, cudaMemcpyHostToDevice, s));
+    LDB_CUDA(cudaMemcpyAsync(d->off.p, h.off.data(), sizeof(long long) * (h.n_rows + 1), cudaMemcpyHostToDevice, s));
+    LDB_CUDA(cudaMemcpyAsync(d->coords.p, coords, sizeof(double) * 3 * n_total, cudaMemcpyHostToDevice, s));
+    RowArgs a;
+    a.n_rows = rows;
+    a.species = d->species.as<int>();
+    a.nbl = d->nbl.as<int>();
+    a.off = d->off.as<long long>();
+    a.max_neigh = std::max(h.maxn, 1);
+    a.coords = d->coords.as<double>();
+    a.n_total = n_total;
+    a.status = d->status.as<int>();
+    std::vector<int> centre, list;
+    if (jac_width > 0) {
+        centre.resize(rows);
+        list.resize(rows);
+        for (int r = 0; r < rows; ++r) {
+            const int base = r / jac_width;
+            list[r] = base;
+            centre[r] = h.centre.empty() ? base : h.centre[base];
+        }
+    } else if (!h.centre.empty()) {
+        centre = h.centre;
+    }
+    if (!centre.empty()) {
+        if ((rc = d->centre.ensure(sizeof(int) * rows))) return rc;
+        LDB_CUDA(cudaMemcpyAsync(d->centre.p, centre.data(), sizeof(int) * rows, cudaMemcpyHostToDevice, s));
+        a.row_centre = d->centre.as<int>();
+    }
+    if (!list.empty()) {
+        if ((rc = d->list.ensure(sizeof(int) * rows))) return rc;
+        LDB_CUDA(cudaMemcpyAsync(d->list.p, list.data(), sizeof(int) * rows, cudaMemcpyHostToDevice, s));
+        a.row_list = d->list.as<int>();
+    }
+    std::vector<double> onehot;
+    if (desc || !dE) {
+        if ((rc = d->desc.ensure(sizeof(double) * std::max<size_t>((size_t)rows * W, 1)))) return rc;
+        a.desc = d->desc.as<double>();
+    }
+    if (dE) {
+        const size_t ndc = jac_width > 0 ? (size_t)rows * 3 * n_total : (size_t)3 * n_total;
+        if ((rc = d->dE.ensure(sizeof(double) * std::max<size_t>((size_t)rows * W, 1))) ||
+            (rc = d->dc.ensure(sizeof(double) * std::max<size_t>(ndc, 1))))
+            return rc;
+        if (jac_width > 0) {
+            onehot.assign((size_t)rows * W, 0.0);
+            for (int r = 0; r < rows; ++r) onehot[(size_t)r * W + (r % jac_width)] = 1.0;
+            LDB_CUDA(cudaMemcpyAsync(d->dE.p, onehot.data(), sizeof(double) * onehot.size(), cudaMemcpyHostToDevice, s));
+            a.dc_stride = 3LL * n_total;
+        } else if (rows > 0) {
+            LDB_CUDA(cudaMemcpyAsync(d->dE.p, dE, sizeof(double) * (size_t)rows * W, cudaMemcpyHostToDevice, s));
+        }
+        LDB_CUDA(cudaMemsetAsync(d->dc.p, 0, sizeof(double) * ndc, s));
+        a.dE = d->dE.as<double>();
+        a.dcoords = d->dc.as<double>();
+        if (jac_width > 0) a.desc = nullptr;
+    }
+    if (rows > 0 && (rc = launch_rows(d, a, s))) return rc;
+    if (dE) {
+        const size_t ndc = jac_width > 0 ? (size_t)rows * 3 * n_total : (size_t)3 * n_total;
+        LDB_CUDA(cudaMemcpyAsync(dcoords, d->dc.p, sizeof(double) * ndc, cudaMemcpyDeviceToHost, s));
+    }
+    if (desc && a.desc && rows > 0)
+        LDB_CUDA(cudaMemcpyAsync(desc, d->desc.p, sizeof(double) * (size_t)rows * W, cudaMemcpyDeviceToHost, s));
+    LDB_CUDA(cudaStreamSynchronize(s));
+    return read_status(d, s);
+}
+
+static void batch_centres(int n_configs, const int *n_atoms, const int *config_ptr, std::vector<int> &c) {
+    c.clear();
+    for (int k = 0; k < n_configs; ++k)
+        for (int j = 0; j < n_atoms[k]; ++j) c.push_back(j + config_ptr[k]);
+}
+
+// ------------------------------------------------------- parameter files
+// FileIOUtils semantics (include/file_io_utils.hpp): data lines skip blank
+// lines and lines whose first character is '#'; numbers are read from the
+// whitespace tokens that parse as numbers (a leading numeric prefix counts).
+struct LineReader {
+    std::ifstream f;
+    bool next(std::string &line) {
+        line.clear();
+        while (line.empty() || line[0] == '#') {
+            if (!std::getline(f, line)) return false;
+        }
+        return true;
+    }
+};
+static bool tok_ints(const std::string &line, int n, std::vector<int> &out) {
+    std::stringstream ss(line);
+    std::string t;
+    out.clear();
+    while ((int)out.size() < n && (ss >> t)) {
+        try {
+            out.push_back(std::stoi(t));
+        } catch (...) {
+        }
+    }
+    return (int)out.size() == n;
+}
+static bool tok_doubles(const std::string &line, int n, std::vector<double> &out) {
+    std::stringstream ss(line);
+    std::string t;
+    out.clear();
+    while ((int)out.size() < n && (ss >> t)) {
+        try {
+            out.push_back(std::stod(t));
+        } catch (...) {
+        }
+    }
+    return (int)out.size() == n;
+}
+static bool tok_strings(const std::string &line, int n, std::vector<std::string> &out) {
+    std::stringstream ss(line);
+    std::string t;
+    out.clear();
+    while ((int)out.size() < n && (ss >> t)) out.push_back(t);
+    return (int)out.size() == n;
+}
+
+// Species block shared by both formats: n_species lines "A B rcut".  The
+// reference reads exactly n_species such lines and orders species names
+// as a sorted set (src/SymmetryFunctions.cpp:302-324).
+static int parse_species(LineReader &lr, int n_species, std::vector<std::string> &species,
+                         std::vector<double> &cutoff) {
+    std::map<std::pair<std::string, std::string>, double> pc;
+    std::set<std::string> names;
+    std::string line;
+    std::vector<std::string> s;
+    std::vector<double> v;
+    for (int k = 0; k < n_species; ++k) {
+        if (!lr.next(line) || !tok_strings(line, 2, s) || !tok_doubles(line, 1, v))
+            return fail(LD_ERR_PARSE, "parameter file: bad species cutoff line");
+        names.insert(s[0]);
+        names.insert(s[1]);
+        pc[{s[0], s[1]}] = v[0];
+        pc[{s[1], s[0]}] = v[0];
+    }
+    species.assign(names.begin(), names.end());
+    const int ns = n_species;
+    cutoff.assign((size_t)ns * ns, 0.0);
+    for (int a = 0; a < ns; ++a)
+        for (int b = 0; b < ns; ++b) {
+            if (a >= (int)species.size() || b >= (int)species.size()) continue;
+            auto it = pc.find({species[a], species[b]});
+            cutoff[(size_t)a * ns + b] = it == pc.end() ? 0.0 : it->second;
+        }
+    return LD_OK;
+}
+
+static int parse_file(ld_descriptor *d, const char *path, int kind) {
+    LineReader lr;
+    lr.f.open(path);
+    if (!lr.f.is_open()) return fail(LD_ERR_PARSE, std::string("Could not open file: ") + path);
+    std::string line;
+    std::vector<int> iv;
+    std::vector<double> dv;
+    std::vector<std::string> sv;
+    if (!lr.next(line) || !tok_strings(line, 1, sv)) return fail(LD_ERR_PARSE, "parameter file: cutoff type");
+    if (!lr.next(line) || !tok_ints(line, 1, iv) || iv[0] <= 0) return fail(LD_ERR_PARSE, "parameter file: number of species");
+    const int ns = iv[0];
+    std::vector<std::string> species;
+    std::vector<double> cutoff;
+    int rc = parse_species(lr, ns, species, cutoff);
+    if (rc) return rc;
+    if (kind == LD_KIND_SYMMETRY_FUNCTIONS) {
+        // src/SymmetryFunctions.cpp:326-406.  The parameter vector is shared
+        // across types and never cleared, and each type's block is read from
+        // the START of that vector -- reproduced as is.
+        if (!lr.next(line) || !tok_ints(line, 1, iv)) return fail(LD_ERR_PARSE, "parameter file: number of types");
+        const int nt = iv[0];
+        std::vector<std::string> names;
+        std::vector<int> codes, sizes;
+        std::vector<double> acc;
+        std::map<std::string, std::vector<double>> per_type;
+        std::map<std::string, std::pair<int, int>> type_sizes;
+        for (int t = 0; t < nt; ++t) {
+            if (!lr.next(line) || !tok_strings(line, 1, sv) || !tok_ints(line, 2, iv))
+                return fail(LD_ERR_PARSE, "parameter file: symmetry-function type line");
+            names.push_back(sv[0]);
+            type_sizes[sv[0]] = {iv[0], iv[1]};
+            for (int r = 0; r < iv[0]; ++r) {
+                if (!lr.next(line) || !tok_doubles(line, iv[1], dv)) return fail(LD_ERR_PARSE, "parameter file: parameter row");
+                acc.insert(acc.end(), dv.begin(), dv.end());
+                per_type[sv[0]] = acc;
+            }
+        }
+        if (!lr.next(line)) return fail(LD_ERR_PARSE, "parameter file: normalize flag");
+        if (!lr.next(line) || !tok_ints(line, 1, iv)) return fail(LD_ERR_PARSE, "parameter file: descriptor size");
+        std::vector<double> params;
+        for (auto &nm : names) {
+            int code = 0;
+            if (nm == "g1") code = 1;
+            else if (nm == "g2") code = 2;
+            else if (nm == "g3") code = 3;
+            else if (nm == "g4") code = 4;
+            else if (nm == "g5") code = 5;
+            if (!code) return fail(LD_ERR_PARSE, "parameter file: unknown symmetry function " + nm);
+            const auto sz = type_sizes[nm];
+            codes.push_back(code);
+            sizes.push_back(sz.first);
+            sizes.push_back(sz.second);
+            const auto &src = per_type[nm];
+            const size_t need = (size_t)sz.first * sz.second;
+            if (src.size() < need) return fail(LD_ERR_PARSE, "parameter file: too few parameters");
+            params.insert(params.end(), src.begin(), src.begin() + need);
+        }
+        return build_sf(d, ns, cutoff.data(), (int)codes.size(), codes.data(), sizes.data(), params.data());
+    }
+    if (kind == LD_KIND_BISPECTRUM) {
+        // src/Bispectrum.cpp:909-1006: jmax (doubled), rfac0, diagonalstyle,
+        // rmin0, switch flag, bzero flag, one weight per species
+        int jmax, style, sw, bz;
+        double rfac0, rmin0;
+        if (!lr.next(line) || !tok_ints(line, 1, iv)) return fail(LD_ERR_PARSE, "parameter file: jmax");
+        jmax = iv[0];
+        if (!lr.next(line) || !tok_doubles(line, 1, dv)) return fail(LD_ERR_PARSE, "parameter file: rfac0");
+        rfac0 = dv[0];
+        if (!lr.next(line) || !tok_ints(line, 1, iv)) return fail(LD_ERR_PARSE, "parameter file: diagonalstyle");
+        style = iv[0];
+        if (!lr.next(line) || !tok_doubles(line, 1, dv)) return fail(LD_ERR_PARSE, "parameter file: rmin0");
+        rmin0 = dv[0];
+        if (!lr.next(line) || !tok_ints(line, 1, iv)) return fail(LD_ERR_PARSE, "parameter file: switch flag");
+        sw = iv[0];
+        if (!lr.next(line) || !tok_ints(line, 1, iv)) return fail(LD_ERR_PARSE, "parameter file: bzero flag");
+        bz = iv[0];
+        if (!lr.next(line) || !tok_doubles(line, (int)species.size(), dv)) return fail(LD_ERR_PARSE, "parameter file: weights");
+        std::vector<double> w(ns, 0.0);
+        for (int k = 0; k < ns && k < (int)dv.size(); ++k) w[k] = dv[k];
+        return build_bs(d, rfac0, 2 * jmax, style, rmin0, sw, bz, ns, cutoff.data(), w.data());
+    }
+    return fail(LD_ERR_INVALID_KIND, "descriptor kind " + std::to_string(kind) + " is not supported (SOAP and Xi are out of scope)");
+}
+
+}  // namespace ldb
+
+// ======================================================================
+// C ABI
+// ======================================================================
+using namespace ldb;
+
+extern "C" {
+
+const char *ld_error_message(void) { return g_err.c_str(); }
+int ld_version(void) { return 10000 * 0 + 100 * 1 + 0; }
+long long ld_launch_count(void) { return g_launches.load(); }
+
+static int new_handle(ld_descriptor **out) {
+    if (!out) return fail(LD_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    int rc = check_device();
+    if (rc) return rc;
+    auto *d = new (std::nothrow) ld_descriptor;
+    if (!d) return fail(LD_ERR_OOM, "host allocation failed");
+    cudaGetDevice(&d->device);
+    *out = d;
+    return LD_OK;
+}
+
+int ld_create_symmetry_functions(ld_descriptor **out, int n_species, const double *cutoff_matrix, int n_types,
+                                 const int *type_codes, const int *sizes, const double *params) {
+    int rc = new_handle(out);
+    if (rc) return rc;
+    rc = build_sf(*out, n_species, cutoff_matrix, n_types, type_codes, sizes, params);
+    if (rc) {
+        delete *out;
+        *out = nullptr;
+    }
+    return rc;
+}
+
+int ld_create_bispectrum(ld_descriptor **out, double rfac0, int twojmax, int diagonalstyle, int use_shared_arrays,
+                         double rmin0, int switch_flag, int bzero_flag, int n_species, const double *cutoff_matrix,
+                         const double *weights) {
+    (void)use_shared_arrays;
+    int rc = new_handle(out);
+    if (rc) return rc;
+    rc = build_bs(*out, rfac0, twojmax, diagonalstyle, rmin0, switch_flag, bzero_flag, n_species, cutoff_matrix,
+                  weights);
+    if (rc) {
+        delete *out;
+        *out = nullptr;
+    }
+    return rc;
+}
+
+int ld_create_from_file(ld_descriptor **out, const char *path, int kind) {
+    if (!path) return fail(LD_ERR_INVALID_ARG, "path is NULL");
+    if (kind != LD_KIND_SYMMETRY_FUNCTIONS && kind != LD_KIND_BISPECTRUM)
+        return fail(LD_ERR_INVALID_KIND, "descriptor kind " + std::to_string(kind) + " is not supported (SOAP and Xi are out of scope)");
+    int rc = new_handle(out);
+    if (rc) return rc;
+    rc = parse_file(*out, path, kind);
+    if (rc) {
+        delete *out;
+        *out = nullptr;
+    }
+    return rc;
+}
+
+int ld_destroy(ld_descriptor *d) {
+    if (!d) return LD_OK;
+    if (d->stream) cudaStreamDestroy(d->stream);
+    delete d;
+    return LD_OK;
+}
+
+int ld_width(const ld_descriptor *d, int *width) {
+    if (!d || !width) return fail(LD_ERR_INVALID_ARG, "NULL argument");
+    *width = d->width;
+    return LD_OK;
+}
+
+int ld_kind(const ld_descriptor *d, int *kind) {
+    if (!d || !kind) return fail(LD_ERR_INVALID_ARG, "NULL argument");
+    *kind = d->kind;
+    return LD_OK;
+}
+
+int ld_compute(ld_descriptor *d, int n_atoms, int n_total, const int *species, const int *neighbor_list,
+               const int *number_of_neighs, const double *coords, double *desc) {
+    if (n_atoms < 0 || (n_atoms > 0 && !number_of_neighs)) return fail(LD_ERR_INVALID_ARG, "bad n_atoms / counts");
+    HostRows h;
+    int rc = make_rows(n_atoms, number_of_neighs, h);
+    if (rc) return rc;
+    return host_pass(d, h, n_total, species, neighbor_list, coords, nullptr, nullptr, desc);
+}
+
+int ld_gradient(ld_descriptor *d, int n_atoms, int n_total, const int *species, const int *neighbor_list,
+                const int *number_of_neighs, const double *coords, const double *dE_ddesc, double *d_coords,
+                double *desc_out) {
+    if (n_atoms < 0 || (n_atoms > 0 && (!number_of_neighs || !dE_ddesc)))
+        return fail(LD_ERR_INVALID_ARG, "bad n_atoms / counts / dE_ddesc");
+    HostRows h;
+    int rc = make_rows(n_atoms, number_of_neighs, h);
+    if (rc) return rc;
+    static const double dummy = 0.0;
+    return host_pass(d, h, n_total, species, neighbor_list, coords, dE_ddesc ? dE_ddesc : &dummy, d_coords, desc_out);
+}
+
+int ld_compute_batch(ld_descriptor *d, int n_configs, const int *n_atoms, const int *config_ptr, int n_total,
+                     const int *species, const int *neighbor_list, const int *number_of_neighs, const double *coords,
+                     double *desc) {
+    if (n_configs < 0 || (n_configs > 0 && (!n_atoms || !config_ptr)))
+        return fail(LD_ERR_INVALID_ARG, "bad configuration arrays");
+    HostRows h;
+    batch_centres(n_configs, n_atoms, config_ptr, h.centre);
+    const int rows = (int)h.centre.size();
+    if (rows > 0 && !number_of_neighs) return fail(LD_ERR_INVALID_ARG, "number_of_neighs is NULL");
+    std::vector<int> keep = h.centre;
+    int rc = make_rows(rows, number_of_neighs, h);
+    if (rc) return rc;
+    h.centre = keep;
+    return host_pass(d, h, n_total, species, neighbor_list, coords, nullptr, nullptr, desc);
+}
+
+int ld_gradient_batch(ld_descriptor *d, int n_configs, const int *n_atoms, const int *config_ptr, int n_total,
+                      const int *species, const int *neighbor_list, const int *number_of_neighs, const double *coords,
+                      const double *dE_ddesc, double *d_coords, double *desc_out) {
+    if (n_configs < 0 || (n_configs > 0 && (!n_atoms || !config_ptr)))
+        return fail(LD_ERR_INVALID_ARG, "bad configuration arrays");
+    HostRows h;
+    batch_centres(n_configs, n_atoms, config_ptr, h.centre);
+    const int rows = (int)h.centre.size();
+    if (rows > 0 && (!number_of_neighs || !dE_ddesc)) return fail(LD_ERR_INVALID_ARG, "NULL counts / dE_ddesc");
+    std::vector<int> keep = h.centre;
+    int rc = make_rows(rows, number_of_neighs, h);
+    if (rc) return rc;
+    h.centre = keep;
+    static const double dummy = 0.0;
+    return host_pass(d, h, n_total, species, neighbor_list, coords, dE_ddesc ? dE_ddesc : &dummy, d_coords, desc_out);
+}
+
+int ld_compute_single_atom(ld_descriptor *d, int index, int n_total, const int *species, const int *neighbors,
+                           int n_neigh, const double *coords, double *desc) {
+    if (n_neigh < 0) return fail(LD_ERR_INVALID_ARG, "n_neigh < 0");
+    HostRows h;
+    int rc = make_rows(1, &n_neigh, h);
+    if (rc) return rc;
+    h.centre = {index};
+    return host_pass(d, h, n_total, species, neighbors, coords, nullptr, nullptr, desc);
+}
+
+int ld_gradient_single_atom(ld_descriptor *d, int index, int n_total, const int *species, const int *neighbors,
+                            int n_neigh, const double *coords, const double *dE_ddesc, double *d_coords,
+                            double *desc_out) {
+    if (n_neigh < 0 || !dE_ddesc) return fail(LD_ERR_INVALID_ARG, "bad n_neigh / dE_ddesc");
+    HostRows h;
+    int rc = make_rows(1, &n_neigh, h);
+    if (rc) return rc;
+    h.centre = {index};
+    return host_pass(d, h, n_total, species, neighbors, coords, dE_ddesc, d_coords, desc_out);
+}
+
+int ld_jacobian(ld_descriptor *d, int n_atoms, int n_total, const int *species, const int *neighbor_list,
+                const int *number_of_neighs, const double *coords, double *J) {
+    if (!d) return fail(LD_ERR_INVALID_ARG, "descriptor handle is NULL");
+    if (n_atoms < 0 || (n_atoms > 0 && (!number_of_neighs || !J))) return fail(LD_ERR_INVALID_ARG, "bad arguments");
+    HostRows h;
+    int rc = make_rows(n_atoms, number_of_neighs, h);
+    if (rc) return rc;
+    static const double dummy = 0.0;
+    return host_pass(d, h, n_total, species, neighbor_list, coords, &dummy, J, nullptr, d->width);
+}
+
+int ld_neighbor_offsets_dev(ld_descriptor *d, int n_rows, const int *number_of_neighs, long long *neigh_offsets,
+                            int *max_neigh, ld_stream stream) {
+    if (!d || n_rows < 0 || !neigh_offsets || (n_rows > 0 && !number_of_neighs))
+        return fail(LD_ERR_INVALID_ARG, "ld_neighbor_offsets_dev: bad arguments");
+    std::lock_guard<std::mutex> lk(d->mu);
+    cudaStream_t s = (cudaStream_t)stream;
+    size_t tb = offsets_tmp_bytes(std::max(n_rows, 1));
+    int rc = d->tmp.ensure(tb + 256);
+    if (rc) return rc;
+    int *dmax = max_neigh ? reinterpret_cast<int *>(static_cast<char *>(d->tmp.p) + tb) : nullptr;
+    rc = offsets_launch(n_rows, number_of_neighs, neigh_offsets, dmax, d->tmp.p, tb, s);
+    if (rc) return rc;
+    if (max_neigh) {
+        LDB_CUDA(cudaMemcpyAsync(max_neigh, dmax, sizeof(int), cudaMemcpyDeviceToHost, s));
+        LDB_CUDA(cudaStreamSynchronize(s));
+    }
+    return LD_OK;
+}
+
+static int dev_pass(ld_descriptor *d, int n_rows, const int *row_centre, const int *species, const int *nbl,
+                    const long long *off, int max_neigh, const double *coords, double *desc, const double *dE,
+                    double *dcoords, const int *image, ld_stream stream) {
+    if (!d) return fail(LD_ERR_INVALID_ARG, "descriptor handle is NULL");
+    if (n_rows < 0 || max_neigh < 0) return fail(LD_ERR_INVALID_ARG, "negative size");
+    if (n_rows == 0) return LD_OK;
+    if (!species || !off || !coords || (!nbl && max_neigh > 0)) return fail(LD_ERR_INVALID_ARG, "NULL device array");
+    if (dE && !dcoords) return fail(LD_ERR_INVALID_ARG, "d_coords is NULL");
+    if (!dE && !desc) return fail(LD_ERR_INVALID_ARG, "desc is NULL");
+    int rc = ensure_status(d);
+    if (rc) return rc;
+    RowArgs a;
+    a.n_rows = n_rows;
+    a.row_centre = row_centre;
+    a.species = species;
+    a.nbl = nbl;
+    a.off = off;
+    a.max_neigh = std::max(max_neigh, 1);
+    a.coords = coords;
+    a.desc = desc;
+    a.dE = dE;
+    a.dcoords = dcoords;
+    a.image = image;
+    a.status = d->status.as<int>();
+    return launch_rows(d, a, (cudaStream_t)stream);
+}
+
+int ld_compute_dev(ld_descriptor *d, int n_rows, const int *row_centre, const int *species, const int *neighbor_list,
+                   const long long *neigh_offsets, int max_neigh, const double *coords, double *desc,
+                   ld_stream stream) {
+    return dev_pass(d, n_rows, row_centre, species, neighbor_list, neigh_offsets, max_neigh, coords, desc, nullptr,
+                    nullptr, nullptr, stream);
+}
+
+int ld_gradient_dev(ld_descriptor *d, int n_rows, const int *row_centre, const int *species,
+                    const int *neighbor_list, const long long *neigh_offsets, int max_neigh, const double *coords,
+                    const double *dE_ddesc, double *d_coords, double *desc_out, const int *image, ld_stream stream) {
+    if (n_rows > 0 && !dE_ddesc) return fail(LD_ERR_INVALID_ARG, "dE_ddesc is NULL");
+    return dev_pass(d, n_rows, row_centre, species, neighbor_list, neigh_offsets, max_neigh, coords, desc_out,
+                    dE_ddesc, d_coords, image, stream);
+}
+
+int ld_sync_status(ld_descriptor *d, ld_stream stream) {
+    if (!d) return fail(LD_ERR_INVALID_ARG, "descriptor handle is NULL");
+    cudaStream_t s = (cudaStream_t)stream;
+    LDB_CUDA(cudaStreamSynchronize(s));
+    return read_status(d, s);
+}
+
+// introspection for tests and the roofline accounting (not in the public
+// header: declared by the Python binding only)
+int ld_bs_info(const ld_descriptor *d, long long *inner_fwd, long long *inner_vjp, int *tasks_fwd, int *tasks_vjp,
+               int *nU, int *nL, int *ntrip, int *nZ) {
+    if (!d || d->kind != LD_KIND_BISPECTRUM) return fail(LD_ERR_INVALID_KIND, "not a bispectrum descriptor");
+    if (inner_fwd) *inner_fwd = d->bs_inner_fwd;
+    if (inner_vjp) *inner_vjp = d->bs_inner_vjp;
+    if (tasks_fwd) *tasks_fwd = d->bs_tasks_fwd;
+    if (tasks_vjp) *tasks_vjp = d->bs_tasks_vjp;
+    if (nU) *nU = d->bs.nU;
+    if (nL) *nL = d->bs.nL;
+    if (ntrip) *ntrip = d->bs.ntrip;
+    if (nZ) *nZ = d->bs.nZall;
+    return LD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,125 @@
+// ld_internal.h -- shared declarations of the libdescriptor_b200 native core.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "libdescriptor_b200.h"
+
+namespace ldb {
+
+// ---------------------------------------------------------------- errors
+void set_error(const std::string &msg);
+int fail(int code, const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+
+#define LDB_CUDA(expr)                                          \
+    do {                                                        \
+        cudaError_t _e = (expr);                                \
+        if (_e != cudaSuccess) return ::ldb::cuda_fail(_e, #expr); \
+    } while (0)
+
+// Device-side error word: kernels raise a status with atomicCAS (first one
+// wins) and the host reads it through ld_sync_status.
+enum DeviceStatus : int {
+    kDevOk = 0,
+    kDevCapacity = 1,   // a row exceeded max_neigh
+    kDevBadIndex = 2,   // neighbour / centre index outside coords
+};
+
+// Launch accounting (all kernels of the library).
+void count_launch(int n = 1);
+
+// ------------------------------------------------------------- device buf
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t n);   // grow-only
+    void release();
+    template <class T> T *as() const { return static_cast<T *>(p); }
+    ~DevBuf() { release(); }
+};
+
+// ------------------------------------------------------ symmetry functions
+// Device view of the parameter tables (outputs re-ordered for the kernel:
+// two-body outputs, then three-body outputs sorted by (type, eta) so that
+// consecutive outputs can share one exp()).
+struct SFDev {
+    int ns = 0, width = 0;
+    int n2 = 0, n3 = 0;
+    const double *rcut = nullptr;   // ns*ns
+    const int *o2 = nullptr;        // output index
+    const int *t2 = nullptr;        // 1..3
+    const double *a2 = nullptr;     // eta (g2) / kappa (g3)
+    const double *b2 = nullptr;     // Rs (g2)
+    const int *o3 = nullptr;        // output index
+    const int *t3 = nullptr;        // 4 / 5
+    const double *P3 = nullptr;     // 2^(1-zeta)
+    const double *z3 = nullptr;     // zeta
+    const double *l3 = nullptr;     // lambda
+    const double *e3 = nullptr;     // eta
+    const int *zi3 = nullptr;       // integer zeta (>=0) or -1
+};
+
+// ------------------------------------------------------------- bispectrum
+struct BSDev {
+    int J = 0, style = 3, switch_flag = 1, bzero_flag = 0, ns = 0;
+    int ncoeff = 0, nU = 0, nL = 0, ntrip = 0, nZall = 0;
+    double rfac0 = 0, rmin0 = 0, wself = 1.0;
+    const double *rcut_flat = nullptr;  // per neighbour species (reference quirk)
+    const double *wj = nullptr;         // per species weight
+    const double *bzero = nullptr;      // J+1
+    const double *rootpq = nullptr;     // (J+1)^2, [p*(J+1)+q] = sqrt(p/q)
+    const int *ublock = nullptr;        // J+2: full-matrix layer offsets
+    const int *lblock = nullptr;        // J+2: left-half layer offsets
+    const int4 *trip = nullptr;         // (j1, j2, j, zoff)
+    const int *cgoff = nullptr;         // per triple
+    const double *cg = nullptr;
+    const int *otrip = nullptr;         // per output: triple index
+    const int *moff = nullptr;          // per triple CSR into (mo, mcoef)
+    const int *mo = nullptr;
+    const double *mcoef = nullptr;
+    const int *jtoff = nullptr;         // J+2: triples with third index j
+    const int *jtlist = nullptr;
+    const int *lel = nullptr;           // nL: packed (j, ma, mb) of left element
+    const int *toff_f = nullptr;        // NT+1 per-thread task offsets (forward)
+    const int4 *task_f = nullptr;
+    const int *toff_v = nullptr;        // NT+1 (gradient: all needed triples)
+    const int4 *task_v = nullptr;
+};
+
+constexpr int kBSThreads = 128;   // threads per bispectrum CTA (one centre)
+constexpr int kSFThreads = 128;   // threads per symmetry-function CTA (4 centres)
+constexpr int kMaxTwoJ = 10;
+
+// ----------------------------------------------------------- launch args
+struct RowArgs {
+    int n_rows = 0;
+    const int *row_centre = nullptr;   // nullable: centre == row
+    const int *row_list = nullptr;     // nullable: neighbour row == row
+    const int *species = nullptr;
+    const int *nbl = nullptr;
+    const long long *off = nullptr;
+    int max_neigh = 0;
+    const double *coords = nullptr;
+    int n_total = 0;                   // 0 = unknown (no index check)
+    double *desc = nullptr;            // nullable for gradient
+    const double *dE = nullptr;        // nullptr = forward only
+    double *dcoords = nullptr;
+    long long dc_stride = 0;           // doubles between rows' gradients (0 = shared)
+    const int *image = nullptr;
+    int *status = nullptr;             // device error word
+};
+
+int sf_launch(const SFDev &p, const RowArgs &a, cudaStream_t s);
+int bs_launch(const BSDev &p, const RowArgs &a, cudaStream_t s);
+size_t bs_smem_bytes(const BSDev &p, int max_neigh, bool vjp);
+
+int offsets_launch(int n_rows, const int *counts, long long *off, int *maxn,
+                   void *tmp, size_t tmp_bytes, cudaStream_t s);
+size_t offsets_tmp_bytes(int n_rows);
+
+}  // namespace ldb

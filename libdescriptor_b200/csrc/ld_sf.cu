@@ -1,0 +1,387 @@
+// ld_sf.cu -- Behler symmetry functions on sm_100a: forward and fused
+// forward + VJP.
+//
+// Semantics follow SymmetryFunctions::compute (src/SymmetryFunctions.cpp:
+// 141-259) and sym_g1..g5 / cut_cos (:67-139): pair terms for every
+// neighbour with r_ij <= rc_ij, triplet terms for kk > jj with r_ik <= rc_ik,
+// g4 additionally zero when r_jk > rc_jk, base <= 0 -> 0.
+//
+// Mapping: one warp owns one centre row.  The row's neighbours (absolute
+// coordinates, distance, cutoff function, species, index) are staged once in
+// the warp's slice of shared memory; lanes then stride over pairs and over
+// the flattened upper triangle of (jj, kk) triplets.  Per-output sums live in
+// registers (one accumulator per output and lane) and are reduced with warp
+// shuffles.  Three-body outputs are pre-sorted by (type, eta) on the host so
+// consecutive outputs reuse one exp().  The gradient kernel recomputes every
+// term, folds the upstream dL/dG into three scalar sums per triplet and
+// type, assembles d/dr_j, d/dr_k, d/dr_i from them, accumulates neighbour
+// gradients in shared memory and scatters them with FP64 atomics (optionally
+// straight onto the ghost's master row).
+#include "ld_internal.h"
+
+namespace ldb {
+namespace {
+
+constexpr double kPi = 3.1415926535897932;
+
+__device__ __forceinline__ void raise_status(int *status, int code) {
+    if (status) atomicCAS(status, 0, code);
+}
+
+__device__ __forceinline__ double cutc(double r, double rc) {
+    return (r < rc) ? 0.5 * (cos(kPi * r / rc) + 1.0) : 0.0;
+}
+__device__ __forceinline__ double dcutc(double r, double rc) {
+    return (r < rc) ? -0.5 * sin(kPi * r / rc) * (kPi / rc) : 0.0;
+}
+__device__ __forceinline__ double ipow(double x, int n) {
+    double r = 1.0;
+    for (int k = 0; k < n; ++k) r *= x;
+    return r;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+struct WarpSlice {
+    double *cx, *cy, *cz, *r, *rc, *fc, *dfc, *gx, *gy, *gz;
+    int *spec, *idx, *inc;
+};
+
+__device__ __forceinline__ WarpSlice slice(double *base, int cap, bool vjp) {
+    WarpSlice s;
+    double *p = base;
+    s.cx = p; p += cap;
+    s.cy = p; p += cap;
+    s.cz = p; p += cap;
+    s.r = p; p += cap;
+    s.rc = p; p += cap;
+    s.fc = p; p += cap;
+    if (vjp) {
+        s.dfc = p; p += cap;
+        s.gx = p; p += cap;
+        s.gy = p; p += cap;
+        s.gz = p; p += cap;
+    } else {
+        s.dfc = s.gx = s.gy = s.gz = nullptr;
+    }
+    int *q = reinterpret_cast<int *>(p);
+    s.spec = q; q += cap;
+    s.idx = q; q += cap;
+    s.inc = q;
+    return s;
+}
+
+template <bool VJP, int M2, int M3>
+__global__ void __launch_bounds__(kSFThreads)
+sf_kernel(SFDev p, RowArgs a, int per_warp_doubles) {
+    extern __shared__ double smem[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int nw = blockDim.x >> 5;
+    const int cap = a.max_neigh;
+    WarpSlice S = slice(smem + (size_t)warp * per_warp_doubles, cap, VJP);
+    const int width = p.width;
+
+    for (int row = blockIdx.x * nw + warp; row < a.n_rows; row += gridDim.x * nw) {
+        const int i = a.row_centre ? a.row_centre[row] : row;
+        const int lrow = a.row_list ? a.row_list[row] : row;
+        const long long off = a.off[lrow];
+        const int n = (int)(a.off[lrow + 1] - off);
+        double *const dco = VJP ? a.dcoords + (size_t)row * a.dc_stride : nullptr;
+        if (n > cap || n < 0 || (a.n_total > 0 && (i < 0 || i >= a.n_total))) {
+            raise_status(a.status, n > cap ? kDevCapacity : kDevBadIndex);
+            if (a.desc)
+                for (int q = lane; q < width; q += 32) a.desc[(size_t)row * width + q] = __longlong_as_double(0x7ff8000000000000LL);
+            continue;
+        }
+        const double cix = a.coords[3 * i], ciy = a.coords[3 * i + 1], ciz = a.coords[3 * i + 2];
+        const int is = a.species[i];
+        // ---- stage the neighbours of this row
+        for (int jj = lane; jj < n; jj += 32) {
+            int j = a.nbl[off + jj];
+            int ok = 1;
+            if (a.n_total > 0 && (j < 0 || j >= a.n_total)) {
+                raise_status(a.status, kDevBadIndex);
+                j = i;   // read in-bounds data; the entry is dropped below
+                ok = 0;
+            }
+            const int js = a.species[j];
+            const double x = a.coords[3 * j], y = a.coords[3 * j + 1], z = a.coords[3 * j + 2];
+            const double rx = x - cix, ry = y - ciy, rz = z - ciz;
+            const double rsq = rx * rx + ry * ry + rz * rz;
+            const double r = sqrt(rsq);
+            const double rc = p.rcut[is * p.ns + js];
+            S.cx[jj] = x;
+            S.cy[jj] = y;
+            S.cz[jj] = z;
+            S.r[jj] = r;
+            S.rc[jj] = rc;
+            S.spec[jj] = js;
+            S.idx[jj] = ok ? j : -1;
+            S.inc[jj] = ok && !(r > rc);
+            S.fc[jj] = cutc(r, rc);
+            if (VJP) {
+                S.dfc[jj] = dcutc(r, rc);
+                S.gx[jj] = 0.0;
+                S.gy[jj] = 0.0;
+                S.gz[jj] = 0.0;
+            }
+        }
+        __syncwarp();
+        const double *dE = VJP ? a.dE + (size_t)row * width : nullptr;
+        double gix = 0.0, giy = 0.0, giz = 0.0;
+        // ---- two-body terms (g1, g2, g3)
+        if (p.n2 > 0) {
+            double acc2[M2];
+#pragma unroll
+            for (int q = 0; q < M2; ++q) acc2[q] = 0.0;
+            for (int jj = lane; jj < n; jj += 32) {
+                if (!S.inc[jj]) continue;
+                const double r = S.r[jj], rc = S.rc[jj], fc = S.fc[jj];
+                double dsum = 0.0;
+#pragma unroll
+                for (int q = 0; q < M2; ++q) {
+                    if (q < p.n2) {
+                        const int t = __ldg(p.t2 + q);
+                        const double pa = __ldg(p.a2 + q), pb = __ldg(p.b2 + q);
+                        double v, dv = 0.0;
+                        if (t == 1) {
+                            v = fc;
+                            if (VJP) dv = S.dfc[jj];
+                        } else if (t == 2) {
+                            const double e = exp(-pa * (r - pb) * (r - pb));
+                            v = e * fc;
+                            if (VJP) dv = e * (-2.0 * pa * (r - pb) * fc + S.dfc[jj]);
+                        } else {
+                            double sn, cs;
+                            sincos(pa * r, &sn, &cs);
+                            v = cs * fc;
+                            if (VJP) dv = -pa * sn * fc + cs * S.dfc[jj];
+                        }
+                        acc2[q] += v;
+                        if (VJP) dsum += __ldg(dE + __ldg(p.o2 + q)) * dv;
+                    }
+                }
+                if (VJP) {
+                    const double inv = 1.0 / r;
+                    const double gx = dsum * (S.cx[jj] - cix) * inv;
+                    const double gy = dsum * (S.cy[jj] - ciy) * inv;
+                    const double gz = dsum * (S.cz[jj] - ciz) * inv;
+                    S.gx[jj] += gx;   // jj is owned by this lane in this phase
+                    S.gy[jj] += gy;
+                    S.gz[jj] += gz;
+                    gix -= gx;
+                    giy -= gy;
+                    giz -= gz;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < M2; ++q) {
+                if (q < p.n2) {
+                    const double v = warp_sum(acc2[q]);
+                    if (lane == 0 && a.desc) a.desc[(size_t)row * width + __ldg(p.o2 + q)] = v;
+                }
+            }
+        }
+        // ---- three-body terms (g4, g5)
+        if (p.n3 > 0) {
+            double acc3[M3];
+#pragma unroll
+            for (int q = 0; q < M3; ++q) acc3[q] = 0.0;
+            int jj = 0, kk = 0;
+            {
+                int rem = lane;
+                while (jj < n - 1 && rem >= n - 1 - jj) {
+                    rem -= n - 1 - jj;
+                    ++jj;
+                }
+                kk = jj + 1 + rem;
+            }
+            __syncwarp();
+            while (jj < n - 1) {
+                if (S.inc[jj]) {
+                    const int ks = S.spec[kk], js = S.spec[jj];
+                    const double rcik = p.rcut[is * p.ns + ks];
+                    const double rcjk = p.rcut[js * p.ns + ks];
+                    const double xk = S.cx[kk], yk = S.cy[kk], zk = S.cz[kk];
+                    const double ikx = xk - cix, iky = yk - ciy, ikz = zk - ciz;
+                    const double jkx = xk - S.cx[jj], jky = yk - S.cy[jj], jkz = zk - S.cz[jj];
+                    const double riksq = ikx * ikx + iky * iky + ikz * ikz;
+                    const double rjksq = jkx * jkx + jky * jky + jkz * jkz;
+                    const double b = sqrt(riksq);
+                    const double d = sqrt(rjksq);
+                    if (!(b > rcik) && S.idx[kk] >= 0) {
+                        const double av = S.r[jj];
+                        const double asq = av * av, bsq = b * b, dsq = d * d;
+                        const double cth = (asq + bsq - dsq) / (2 * av * b);
+                        const double fa = S.fc[jj];
+                        const double fb = cutc(b, rcik);
+                        double fd, dfd = 0.0;
+                        {
+                            const double t = kPi * d / rcjk;
+                            double sn, cs;
+                            sincos(t, &sn, &cs);
+                            fd = (d < rcjk) ? 0.5 * (cs + 1.0) : 0.0;
+                            if (VJP) dfd = (d < rcjk) ? -0.5 * sn * (kPi / rcjk) : 0.0;
+                        }
+                        const bool g4ok = !(d > rcjk);
+                        const double S4 = asq + bsq + dsq, S5 = asq + bsq;
+                        double A4 = 0, B4 = 0, C4 = 0, A5 = 0, B5 = 0, C5 = 0;
+                        double eprev = -1.0, E = 0.0;
+                        int tprev = 0;
+#pragma unroll
+                        for (int q = 0; q < M3; ++q) {
+                            if (q < p.n3) {
+                                const int t = __ldg(p.t3 + q);
+                                if (t == 5 || g4ok) {
+                                    const double eta = __ldg(p.e3 + q);
+                                    if (eta != eprev || t != tprev) {
+                                        E = exp(-eta * (t == 4 ? S4 : S5));
+                                        eprev = eta;
+                                        tprev = t;
+                                    }
+                                    const double lam = __ldg(p.l3 + q);
+                                    const double base = 1.0 + lam * cth;
+                                    const int zi = __ldg(p.zi3 + q);
+                                    const double zeta = __ldg(p.z3 + q);
+                                    double cp = 0.0;
+                                    if (base > 0) cp = zi >= 0 ? ipow(base, zi) : pow(base, zeta);
+                                    const double P = __ldg(p.P3 + q);
+                                    const double v = (t == 4) ? P * cp * E * fa * fb * fd
+                                                              : P * cp * E * fa * fb;
+                                    acc3[q] += v;
+                                    if (VJP && base > 0) {
+                                        const double g = __ldg(dE + __ldg(p.o3 + q));
+                                        const double bq = g * P * E;
+                                        double dcp;
+                                        if (zi >= 0) dcp = zi > 0 ? zeta * ipow(base, zi - 1) : 0.0;
+                                        else dcp = zeta * pow(base, zeta - 1.0);
+                                        if (t == 4) {
+                                            A4 += bq * cp;
+                                            B4 += bq * cp * eta;
+                                            C4 += bq * dcp * lam;
+                                        } else {
+                                            A5 += bq * cp;
+                                            B5 += bq * cp * eta;
+                                            C5 += bq * dcp * lam;
+                                        }
+                                    }
+                                }
+                            }
+                        }
+                        if (VJP) {
+                            const double dfa = S.dfc[jj];
+                            const double dfb = dcutc(b, rcik);
+                            const double dca = (asq - bsq + dsq) / (2 * asq * b);
+                            const double dcb = (bsq - asq + dsq) / (2 * av * bsq);
+                            const double dcd = -d / (av * b);
+                            const double F4 = fa * fb * fd, F5 = fa * fb;
+                            const double Ga = F4 * C4 * dca - 2.0 * av * F4 * B4 + dfa * fb * fd * A4 +
+                                              F5 * C5 * dca - 2.0 * av * F5 * B5 + dfa * fb * A5;
+                            const double Gb = F4 * C4 * dcb - 2.0 * b * F4 * B4 + fa * dfb * fd * A4 +
+                                              F5 * C5 * dcb - 2.0 * b * F5 * B5 + fa * dfb * A5;
+                            const double Gd = F4 * C4 * dcd - 2.0 * d * F4 * B4 + fa * fb * dfd * A4 +
+                                              F5 * C5 * dcd;
+                            const double ia = 1.0 / av, ib = 1.0 / b, id = d > 0 ? 1.0 / d : 0.0;
+                            const double ijx = (S.cx[jj] - cix) * ia, ijy = (S.cy[jj] - ciy) * ia,
+                                         ijz = (S.cz[jj] - ciz) * ia;
+                            const double ukx = ikx * ib, uky = iky * ib, ukz = ikz * ib;
+                            const double udx = jkx * id, udy = jky * id, udz = jkz * id;
+                            atomicAdd(&S.gx[jj], Ga * ijx - Gd * udx);
+                            atomicAdd(&S.gy[jj], Ga * ijy - Gd * udy);
+                            atomicAdd(&S.gz[jj], Ga * ijz - Gd * udz);
+                            atomicAdd(&S.gx[kk], Gb * ukx + Gd * udx);
+                            atomicAdd(&S.gy[kk], Gb * uky + Gd * udy);
+                            atomicAdd(&S.gz[kk], Gb * ukz + Gd * udz);
+                            gix -= Ga * ijx + Gb * ukx;
+                            giy -= Ga * ijy + Gb * uky;
+                            giz -= Ga * ijz + Gb * ukz;
+                        }
+                    }
+                }
+                // advance 32 triplets along the flattened upper triangle
+                int rem = kk - (jj + 1) + 32;
+                while (jj < n - 1 && rem >= n - 1 - jj) {
+                    rem -= n - 1 - jj;
+                    ++jj;
+                }
+                kk = jj + 1 + rem;
+            }
+#pragma unroll
+            for (int q = 0; q < M3; ++q) {
+                if (q < p.n3) {
+                    const double v = warp_sum(acc3[q]);
+                    if (lane == 0 && a.desc) a.desc[(size_t)row * width + __ldg(p.o3 + q)] = v;
+                }
+            }
+        }
+        if (VJP) {
+            __syncwarp();
+            for (int jj = lane; jj < n; jj += 32) {
+                const int j = S.idx[jj];
+                if (j < 0) continue;
+                const int tj = a.image ? a.image[j] : j;
+                atomicAdd(dco + 3 * (size_t)tj, S.gx[jj]);
+                atomicAdd(dco + 3 * (size_t)tj + 1, S.gy[jj]);
+                atomicAdd(dco + 3 * (size_t)tj + 2, S.gz[jj]);
+            }
+            gix = warp_sum(gix);
+            giy = warp_sum(giy);
+            giz = warp_sum(giz);
+            if (lane == 0) {
+                const int ti = a.image ? a.image[i] : i;
+                atomicAdd(dco + 3 * (size_t)ti, gix);
+                atomicAdd(dco + 3 * (size_t)ti + 1, giy);
+                atomicAdd(dco + 3 * (size_t)ti + 2, giz);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+template <bool VJP, int M2, int M3>
+int launch_t(const SFDev &p, const RowArgs &a, cudaStream_t s) {
+    const int cap = a.max_neigh > 0 ? a.max_neigh : 1;
+    const int ndbl = cap * (VJP ? 10 : 6);
+    const int per_warp = ndbl + (3 * cap + 1) / 2 + 2;  // doubles (ints packed after)
+    const size_t per_warp_bytes = (size_t)per_warp * sizeof(double);
+    int nw = 4;
+    while (nw > 1 && per_warp_bytes * nw > 200 * 1024) --nw;
+    if (per_warp_bytes * nw > 220 * 1024)
+        return fail(LD_ERR_CAPACITY, "symmetry functions: max_neigh=" + std::to_string(a.max_neigh) +
+                                         " exceeds the on-chip neighbour staging capacity");
+    const size_t smem = per_warp_bytes * nw;
+    auto kern = sf_kernel<VJP, M2, M3>;
+    LDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int dev = 0, nsm = 148, per_sm = 1;
+    LDB_CUDA(cudaGetDevice(&dev));
+    LDB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    LDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, nw * 32, smem));
+    if (per_sm < 1) per_sm = 1;
+    const int rows_per_block = nw;
+    long long want = (a.n_rows + rows_per_block - 1) / rows_per_block;
+    long long grid = (long long)nsm * per_sm;
+    if (want < grid) grid = want;
+    if (grid < 1) grid = 1;
+    kern<<<(unsigned)grid, nw * 32, smem, s>>>(p, a, per_warp);
+    count_launch();
+    LDB_CUDA(cudaGetLastError());
+    return LD_OK;
+}
+
+}  // namespace
+
+int sf_launch(const SFDev &p, const RowArgs &a, cudaStream_t s) {
+    if (a.n_rows <= 0) return LD_OK;
+    const int m = p.n2 > p.n3 ? p.n2 : p.n3;
+    const bool vjp = a.dE != nullptr;
+    if (m <= 16) return vjp ? launch_t<true, 16, 16>(p, a, s) : launch_t<false, 16, 16>(p, a, s);
+    if (m <= 32) return vjp ? launch_t<true, 32, 32>(p, a, s) : launch_t<false, 32, 32>(p, a, s);
+    if (m <= 64) return vjp ? launch_t<true, 64, 64>(p, a, s) : launch_t<false, 64, 64>(p, a, s);
+    return fail(LD_ERR_CAPACITY, "symmetry functions: more than 64 outputs of one body order");
+}
+
+}  // namespace ldb

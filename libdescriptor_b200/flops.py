@@ -1,0 +1,126 @@
+"""Algorithmic FP64 operation counts per centre atom (roofline numerator).
+
+Convention: add / mul = 1 flop, FMA = 2 flops, complex arithmetic counted as
+written; each library call (exp, sincos, sqrt, divide, tan, pow, cos) costs
+W_op flops, W_op measured on the device (``ld_measure_fp64_op_cost``: the
+FP64-pipe flops that fit in the time of one call).  Work is counted for the
+needed outputs only, along the loops of the kernels:
+
+bispectrum (twojmax J), per in-cutoff neighbour and per computed left-half
+element (j, ma, mb <= j/2; mirror rows of the middle column excluded):
+  U recursion       b-term 8 (ma >= 1) + a-term 10 (ma < j), Utot += 4
+  dU recursion      per direction: b-term 16, a-term 18
+  contraction       20 (S and three V sums)
+per Z element: 10 per (ma1, mb1) term + 4 per ma1 row; B: 4 per element;
+betaj: 2 per map entry; Y: 4 per (element, triple).
+Per neighbour calls: forward sqrt x3, tan, divide x2, cos; gradient adds
+sincos, tan, sqrt x2, divide x3, sin/cos of the switching function.
+
+symmetry functions, per listed neighbour: staging 8 + sqrt + divide + cos;
+per pair output 6 + exp (g2); per triplet 25 + 2 sqrt + 3 divide + 2 cos
+(fb, fd) and per three-body output 12 + one exp per distinct eta; the
+gradient adds 14 per output and 60 + 3 divide per triplet.
+"""
+from __future__ import annotations
+
+from functools import lru_cache
+
+OPS = {"exp": 0, "sincos": 1, "sqrt": 2, "div": 3, "tan": 4, "pow": 5, "cos": 6}
+
+
+def measure_weights(fp64_tflops: float, iters: int = 2048) -> dict:
+    """W_op for every call, measured on the current device."""
+    from . import _libdescriptor as _ext
+
+    return {k: float(_ext._measure_fp64_op_cost(v, iters, fp64_tflops)) for k, v in OPS.items()}
+
+
+DEFAULT_WEIGHTS = {"exp": 20.0, "sincos": 40.0, "sqrt": 12.0, "div": 12.0, "tan": 40.0,
+                   "pow": 60.0, "cos": 30.0}
+
+
+@lru_cache(maxsize=None)
+def _bs_tables(J: int, style: int):
+    """(left elements with their (ma>=1, ma<j) flags, Z work, outputs, triples)."""
+    elems = []
+    for j in range(1, J + 1):
+        h = j // 2
+        for ma in range(j + 1):
+            for mb in range(h + 1):
+                if j % 2 == 0 and mb == h and ma > h:
+                    continue
+                elems.append((ma >= 1, ma < j))
+    outs = []
+    if style == 0:
+        outs = [(a, b, c) for a in range(J + 1) for b in range(a + 1) for c in range(a - b, min(J, a + b) + 1, 2)]
+    elif style == 1:
+        outs = [(a, a, c) for a in range(J + 1) for c in range(0, min(J, 2 * a) + 1, 2)]
+    elif style == 2:
+        outs = [(a, a, a) for a in range(J + 1)]
+    else:
+        outs = [(a, b, c) for a in range(J + 1) for b in range(a + 1)
+                for c in range(a - b, min(J, a + b) + 1, 2) if c >= a]
+    trip_all = [(a, b, c) for a in range(J + 1) for b in range(a + 1) for c in range(a - b, min(J, a + b) + 1, 2)]
+
+    def key(x, y, z):
+        return (max(x, y), min(x, y), z)
+
+    need_v = set(outs)
+    mentries = 0
+    for (a, b, c) in outs:
+        for t in (key(a, b, c), key(c, b, a), key(c, a, b)):
+            need_v.add(t)
+            mentries += 1
+
+    def zwork(trips):
+        terms = rows = nel = 0
+        for (j1, j2, j) in trips:
+            for mb in range(j // 2 + 1):
+                for ma in range(j + 1):
+                    if j % 2 == 0 and mb == j // 2 and ma > j // 2:
+                        continue
+                    na = min(j1, (2 * ma - j + j2 + j1) // 2) - max(0, (2 * ma - j - j2 + j1) // 2) + 1
+                    nb = min(j1, (2 * mb - j + j2 + j1) // 2) - max(0, (2 * mb - j - j2 + j1) // 2) + 1
+                    terms += max(na, 0) * max(nb, 0)
+                    rows += max(na, 0)
+                    nel += 1
+        return terms, rows, nel
+
+    zf = zwork(sorted(set(outs)))
+    zv = zwork(sorted(need_v))
+    b_elems = sum((c + 1) * (c // 2 + 1) for (_, _, c) in outs)
+    y_terms = 0
+    for (j1, j2, j) in sorted(need_v):
+        y_terms += (j + 1) * (j // 2 + 1)
+    return elems, zf, zv, b_elems, len(outs), mentries, y_terms, len(trip_all)
+
+
+def bs_flops_per_atom(J: int, style: int, n_in: float, vjp: bool, w: dict | None = None) -> float:
+    w = w or DEFAULT_WEIGHTS
+    elems, zf, zv, b_elems, nout, mentries, y_terms, _ = _bs_tables(J, style)
+    u_el = sum((8 if b else 0) + (10 if a else 0) + 4 for b, a in elems)
+    per_nb_fwd = u_el + 3 * w["sqrt"] + w["tan"] + 2 * w["div"] + w["cos"] + 20
+    terms, rows, _ = zv if vjp else zf
+    z = 10 * terms + 4 * rows
+    f = n_in * per_nb_fwd + z + 4 * b_elems
+    if vjp:
+        du_el = sum(3 * ((16 if b else 0) + (18 if a else 0)) + 20 + (8 if b else 0) + (10 if a else 0)
+                    for b, a in elems)
+        per_nb_bwd = du_el + w["sincos"] + w["tan"] + 2 * w["sqrt"] + 3 * w["div"] + w["sincos"] + 40
+        f += n_in * per_nb_bwd + 2 * mentries + 4 * y_terms
+    return float(f)
+
+
+def sf_flops_per_atom(n_neigh: float, n_pair_out: int, n_three_out: int, n_eta3: int, vjp: bool,
+                      n_in_pairs: float | None = None, w: dict | None = None) -> float:
+    """n_in_pairs: triplets (jj < kk) whose r_ij and r_ik are inside the cutoff
+    (defaults to all n(n-1)/2)."""
+    w = w or DEFAULT_WEIGHTS
+    trip = n_in_pairs if n_in_pairs is not None else n_neigh * (n_neigh - 1) / 2.0
+    f = n_neigh * (8 + w["sqrt"] + w["div"] + w["cos"])
+    f += n_neigh * n_pair_out * (6 + w["exp"])
+    f += trip * (25 + 2 * w["sqrt"] + 3 * w["div"] + 2 * w["cos"] + n_three_out * 12 + n_eta3 * w["exp"])
+    if vjp:
+        f += n_neigh * (n_pair_out * 8 + w["div"] + 10)
+        f += trip * (n_three_out * 14 + 60 + 3 * w["div"])
+    return float(f)

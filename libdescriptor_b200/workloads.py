@@ -1,0 +1,174 @@
+"""Seeded synthetic inputs: periodic cells, ghost padding and neighbour lists.
+
+The reference measures nothing on a public dataset; these generators build the
+cells its documented use implies (periodic Si diamond supercells, random
+two-species packings) and turn them into the reference's input layout with the
+library's own padding / neighbour-list builder (``create_paddings`` and
+``NeighList``, the KLIFF-derived algorithm of
+python_bindings/neighbor/neighbor_list.cpp).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _libdescriptor as _ext
+
+# 8-atom conventional diamond basis (fractional)
+_DIAMOND = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0],
+                     [.25, .25, .25], [.25, .75, .75], [.75, .25, .75], [.75, .75, .25]])
+
+SF24_G2_ETA = (0.001, 0.005, 0.01, 0.02, 0.04, 0.08, 0.16, 0.32)
+SF24_G4_ETA = (0.001, 0.01, 0.03, 0.08)
+
+
+def sf24_params():
+    """The 24-d Behler set: 8 g2 (Rs = 0) + 16 g4 rows ordered (zeta, lambda, eta)."""
+    g2 = [[e, 0.0] for e in SF24_G2_ETA]
+    g4 = [[z, lam, e] for z in (1.0, 4.0) for lam in (-1.0, 1.0) for e in SF24_G4_ETA]
+    params = [v for row in g2 for v in row] + [v for row in g4 for v in row]
+    return ["g2", "g4"], [8, 2, 16, 3], params
+
+
+def diamond_cell(n1, n2, n3, a=5.43, jitter=0.0, strain=0.0, seed=0):
+    """Si diamond supercell of n1 x n2 x n3 conventional cells.  strain: each
+    cell-matrix entry perturbed by U(-strain, strain) (H = (I + eps) H0)."""
+    rng = np.random.default_rng(seed)
+    h0 = np.diag([n1 * a, n2 * a, n3 * a]).astype(np.float64)
+    eps = rng.uniform(-strain, strain, (3, 3)) if strain else np.zeros((3, 3))
+    cell = h0 @ (np.eye(3) + eps).T  # rows are lattice vectors
+    grid = np.array([[i, j, k] for i in range(n1) for j in range(n2) for k in range(n3)], dtype=np.float64)
+    frac = (grid[:, None, :] + _DIAMOND[None, :, :]).reshape(-1, 3) / np.array([n1, n2, n3])
+    x = frac @ cell
+    if jitter:
+        x = x + rng.normal(0.0, jitter, x.shape)
+    return np.ascontiguousarray(x), np.ascontiguousarray(cell)
+
+
+def random_packing(n, density=0.05, dmin=2.0, n_species=2, seed=0, max_tries=200):
+    """n atoms uniformly in a periodic cube of side (n/density)^(1/3) with a
+    minimum pair distance dmin (random sequential addition by rejection).
+    Species alternate 0,1,... so the mix is 50/50 for two species."""
+    from scipy.spatial import cKDTree
+
+    rng = np.random.default_rng(seed)
+    side = (n / density) ** (1.0 / 3.0)
+    acc = np.zeros((0, 3))
+    tries = 0
+    while acc.shape[0] < n:
+        tries += 1
+        if tries > max_tries:
+            raise RuntimeError("random_packing: could not place all atoms")
+        m = max(64, int(1.3 * (n - acc.shape[0])))
+        cand = rng.uniform(0.0, side, (m, 3))
+        if acc.shape[0]:
+            tree = cKDTree(acc, boxsize=side)
+            d, _ = tree.query(cand, k=1)
+            cand = cand[d >= dmin]
+        if cand.shape[0] == 0:
+            continue
+        ct = cKDTree(cand, boxsize=side)
+        pairs = ct.query_pairs(dmin, output_type="ndarray")
+        keep = np.ones(cand.shape[0], dtype=bool)
+        if pairs.size:
+            # greedy in index order: drop the later member of each close pair
+            order = np.argsort(pairs[:, 0], kind="stable")
+            for a, b in pairs[order]:
+                if keep[a] and keep[b]:
+                    keep[b] = False
+        cand = cand[keep][: n - acc.shape[0]]
+        acc = np.concatenate([acc, cand])
+    species = (np.arange(n) % n_species).astype(np.int32)
+    return np.ascontiguousarray(acc), np.eye(3) * side, species
+
+
+@dataclass
+class Config:
+    """One configuration in the reference's input layout."""
+
+    n_atoms: int
+    coords: np.ndarray          # (n_total, 3): contributing atoms then ghosts
+    species: np.ndarray         # (n_total,) int32
+    image: np.ndarray           # (n_total,) master atom of each row
+    counts: np.ndarray          # (n_atoms,) int32
+    nbl: np.ndarray             # (sum counts,) int32
+    cell: np.ndarray = field(default=None)
+
+    @property
+    def n_total(self) -> int:
+        return int(self.coords.shape[0])
+
+
+def prepare(coords, cell, species, cutoff, pbc=(1, 1, 1)) -> Config:
+    """Ghost padding + full neighbour list within `cutoff` of every
+    contributing atom (reference NeighborList semantics)."""
+    coords = np.ascontiguousarray(coords, dtype=np.float64)
+    species = np.ascontiguousarray(species, dtype=np.int32)
+    n = coords.shape[0]
+    pc, ps, pi = _ext.create_paddings(float(cutoff), np.ascontiguousarray(cell, dtype=np.float64),
+                                      np.asarray(pbc, dtype=np.int32), coords, species)
+    allx = np.ascontiguousarray(np.concatenate([coords, pc]))
+    alls = np.ascontiguousarray(np.concatenate([species, ps]).astype(np.int32))
+    image = np.concatenate([np.arange(n, dtype=np.int32), pi.astype(np.int32)])
+    need = np.zeros(allx.shape[0], dtype=np.int32)
+    need[:n] = 1
+    nl = _ext.NeighList()
+    nl.build(allx, float(cutoff), np.asarray([cutoff], dtype=np.float64), need)
+    counts = np.zeros(n, dtype=np.int32)
+    lists = []
+    cut = np.asarray([cutoff], dtype=np.float64)
+    for i in range(n):
+        c, nb = nl.get_neigh(cut, 0, i)
+        counts[i] = c
+        lists.append(nb)
+    nbl = np.ascontiguousarray(np.concatenate(lists).astype(np.int32)) if lists else np.zeros(0, np.int32)
+    return Config(n, allx, alls, image, counts, nbl, np.asarray(cell))
+
+
+@dataclass
+class Batch:
+    """Concatenated configurations in the compute_batch layout
+    (src/Descriptors.cpp:138-163): centre of row (c, j) is j + config_ptr[c]."""
+
+    n_atoms: np.ndarray
+    config_ptr: np.ndarray
+    coords: np.ndarray
+    species: np.ndarray
+    image: np.ndarray           # global master row of every coordinate row
+    counts: np.ndarray
+    nbl: np.ndarray
+    row_centre: np.ndarray
+    contrib_rows: np.ndarray    # global coordinate row of every centre
+
+    @property
+    def n_rows(self) -> int:
+        return int(self.n_atoms.sum())
+
+
+def concat(configs) -> Batch:
+    n_atoms, ptr, xs, ss, ims, cnts, nbls, centres = [], [], [], [], [], [], [], []
+    base = 0
+    for c in configs:
+        n_atoms.append(c.n_atoms)
+        ptr.append(base)
+        xs.append(c.coords)
+        ss.append(c.species)
+        ims.append(c.image + base)
+        cnts.append(c.counts)
+        nbls.append(c.nbl + base)
+        centres.append(np.arange(c.n_atoms, dtype=np.int32) + base)
+        base += c.n_total
+    rc = np.concatenate(centres).astype(np.int32)
+    return Batch(np.asarray(n_atoms, np.int32), np.asarray(ptr, np.int32),
+                 np.ascontiguousarray(np.concatenate(xs)), np.concatenate(ss).astype(np.int32),
+                 np.concatenate(ims).astype(np.int32), np.concatenate(cnts).astype(np.int32),
+                 np.concatenate(nbls).astype(np.int32), rc, rc)
+
+
+def fold(grad, n_atoms, image):
+    """Ghost rows added onto their masters (the reference's assemble_forces,
+    python_package/libdescriptor/neighbor.py:227-263)."""
+    out = np.array(grad[:n_atoms], dtype=np.float64, copy=True)
+    np.add.at(out, image[n_atoms:], grad[n_atoms:])
+    return out
