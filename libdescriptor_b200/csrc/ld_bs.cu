@@ -395,6 +395,7 @@ __global__ void __launch_bounds__(NT) bs_kernel(BSDev p, RowArgs a, int cap) {
                     const int pk = __ldg(p.lel + e);
                     const int jl = pk & 0xff, ma = (pk >> 8) & 0xff, mb = (pk >> 16) & 0xff;
                     const int nc = jl / 2 + 1;
+                    if ((jl & 1) == 0 && mb == jl / 2 && ma > jl / 2) continue;  // mirror row: unused
                     double yr = 0.0, yi = 0.0;
                     const int q0 = __ldg(p.jtoff + jl), q1 = __ldg(p.jtoff + jl + 1);
                     for (int q = q0; q < q1; ++q) {
