@@ -359,6 +359,11 @@ __global__ void __launch_bounds__(NT) bs_kernel(BSDev p, RowArgs a, int cap) {
             const double *zr = C.scratch, *zi = C.scratch + p.nZall;
             for (int o = tid; o < width; o += NT) {
                 const int t = __ldg(p.otrip + o);
+                if (t < 0) {   // parity-forbidden triple: constant zero output
+                    if (a.desc) a.desc[(size_t)row * width + o] = 0.0;
+                    if (VJP) C.beta[o] = 0.0;
+                    continue;
+                }
                 const int4 tr = __ldg(p.trip + t);
                 const int jl = tr.z, hj = jl / 2, nc = hj + 1, zo = tr.w;
                 const int ub = __ldg(p.ublock + jl);

@@ -298,8 +298,20 @@ static void lpt_schedule(const std::vector<BSTask> &tasks_in, const std::vector<
     toff[nt] = (int)packed.size();
 }
 
+static int build_bs_impl(ld_descriptor *d, double rfac0, int J, int style, double rmin0, int switch_flag,
+                         int bzero_flag, int ns, const double *cutoff, const double *weights);
+
 static int build_bs(ld_descriptor *d, double rfac0, int J, int style, double rmin0, int switch_flag,
                     int bzero_flag, int ns, const double *cutoff, const double *weights) {
+    try {
+        return build_bs_impl(d, rfac0, J, style, rmin0, switch_flag, bzero_flag, ns, cutoff, weights);
+    } catch (const std::exception &e) {
+        return fail(LD_ERR_INVALID_ARG, std::string("bispectrum tables: ") + e.what());
+    }
+}
+
+static int build_bs_impl(ld_descriptor *d, double rfac0, int J, int style, double rmin0, int switch_flag,
+                         int bzero_flag, int ns, const double *cutoff, const double *weights) {
     if (J < 0 || J > kMaxTwoJ)
         return fail(J < 0 ? LD_ERR_INVALID_ARG : LD_ERR_CAPACITY,
                     "bispectrum: twojmax=" + std::to_string(J) + " outside 0.." + std::to_string(kMaxTwoJ));
@@ -359,12 +371,17 @@ static int build_bs(ld_descriptor *d, double rfac0, int J, int style, double rmi
     std::vector<std::array<int, 3>> outs;
     bs_outputs(J, style, outs);
     b.ncoeff = (int)outs.size();
+    // An output whose (j1, j2, j) breaks the parity rule (style 2 with odd
+    // j1) is never written by the reference's compute_bi, so it keeps the
+    // zero its barray was allocated with (src/Bispectrum.cpp:391-427,
+    // 450-454): otrip = -1 marks a constant-zero output.
     std::vector<int> otrip;
     d->bs_out_j1.clear();
     d->bs_out_j2.clear();
     d->bs_out_j.clear();
     for (auto &o : outs) {
-        otrip.push_back(tindex.at(o));
+        auto it = tindex.find(o);
+        otrip.push_back(it == tindex.end() ? -1 : it->second);
         d->bs_out_j1.push_back(o[0]);
         d->bs_out_j2.push_back(o[1]);
         d->bs_out_j.push_back(o[2]);
@@ -378,6 +395,7 @@ static int build_bs(ld_descriptor *d, double rfac0, int J, int style, double rmi
     std::vector<std::map<int, double>> M(trip.size());
     auto tri = [&](int x, int y, int z) { return tindex.at({std::max(x, y), std::min(x, y), z}); };
     for (int o = 0; o < (int)outs.size(); ++o) {
+        if (otrip[o] < 0) continue;
         const int a = outs[o][0], bb = outs[o][1], c = outs[o][2];
         M[tri(a, bb, c)][o] += 1.0;
         M[tri(c, bb, a)][o] += (double)(c + 1) / (a + 1);
@@ -402,7 +420,10 @@ static int build_bs(ld_descriptor *d, double rfac0, int J, int style, double rmi
     jtoff[J + 1] = (int)jtlist.size();
     // Z-element tasks: (triple, ma, mb<=j/2) except the mirror rows of the
     // middle column, which neither B nor Y reads.
-    std::set<int> need_f(otrip.begin(), otrip.end()), need_v = need_f;
+    std::set<int> need_f;
+    for (int t : otrip)
+        if (t >= 0) need_f.insert(t);
+    std::set<int> need_v = need_f;
     for (size_t t = 0; t < trip.size(); ++t)
         if (!M[t].empty()) need_v.insert((int)t);
     auto make_tasks = [&](const std::set<int> &need, long long &inner) {
@@ -535,9 +556,25 @@ static int ensure_status(ld_descriptor *d) {
 // Generic host-buffer pass: stage, launch, copy back.  dE == nullptr means
 // forward only.  dcoords (n_total*3) and desc are overwritten when given.
 // jac_width > 0 turns rows into (centre, component) pairs of a Jacobian.
+static int host_pass_impl(ld_descriptor *d, HostRows &h, int n_total, const int *species, const int *nbl,
+                          const double *coords, const double *dE, double *dcoords, double *desc,
+                          int jac_width);
+
 static int host_pass(ld_descriptor *d, HostRows &h, int n_total, const int *species, const int *nbl,
                      const double *coords, const double *dE, double *dcoords, double *desc,
                      int jac_width = 0) {
+    try {
+        return host_pass_impl(d, h, n_total, species, nbl, coords, dE, dcoords, desc, jac_width);
+    } catch (const std::bad_alloc &) {
+        return fail(LD_ERR_OOM, "host allocation failed");
+    } catch (const std::exception &e) {
+        return fail(LD_ERR_INVALID_ARG, e.what());
+    }
+}
+
+static int host_pass_impl(ld_descriptor *d, HostRows &h, int n_total, const int *species, const int *nbl,
+                          const double *coords, const double *dE, double *dcoords, double *desc,
+                          int jac_width) {
     if (!d) return fail(LD_ERR_INVALID_ARG, "descriptor handle is NULL");
     if (h.n_rows < 0 || n_total < 0) return fail(LD_ERR_INVALID_ARG, "negative size");
     if (h.n_rows > 0 && (!species || !coords || (h.nnz > 0 && !nbl)))
@@ -706,7 +743,17 @@ static int parse_species(LineReader &lr, int n_species, std::vector<std::string>
     return LD_OK;
 }
 
+static int parse_file_impl(ld_descriptor *d, const char *path, int kind);
+
 static int parse_file(ld_descriptor *d, const char *path, int kind) {
+    try {
+        return parse_file_impl(d, path, kind);
+    } catch (const std::exception &e) {
+        return fail(LD_ERR_PARSE, std::string("parameter file: ") + e.what());
+    }
+}
+
+static int parse_file_impl(ld_descriptor *d, const char *path, int kind) {
     LineReader lr;
     lr.f.open(path);
     if (!lr.f.is_open()) return fail(LD_ERR_PARSE, std::string("Could not open file: ") + path);
@@ -967,7 +1014,8 @@ int ld_neighbor_offsets_dev(ld_descriptor *d, int n_rows, const int *number_of_n
         return fail(LD_ERR_INVALID_ARG, "ld_neighbor_offsets_dev: bad arguments");
     std::lock_guard<std::mutex> lk(d->mu);
     cudaStream_t s = (cudaStream_t)stream;
-    size_t tb = offsets_tmp_bytes(std::max(n_rows, 1));
+    // the max lands right after the CUB scratch: keep it 256-byte aligned
+    size_t tb = (offsets_tmp_bytes(std::max(n_rows, 1)) + 255) & ~(size_t)255;
     int rc = d->tmp.ensure(tb + 256);
     if (rc) return rc;
     int *dmax = max_neigh ? reinterpret_cast<int *>(static_cast<char *>(d->tmp.p) + tb) : nullptr;

@@ -65,6 +65,8 @@ def _bs_tables(J: int, style: int):
     def key(x, y, z):
         return (max(x, y), min(x, y), z)
 
+    valid = set(trip_all)
+    outs = [o for o in outs if o in valid]   # parity-forbidden outputs are constant zero
     need_v = set(outs)
     mentries = 0
     for (a, b, c) in outs:
