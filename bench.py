@@ -113,7 +113,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -123,7 +123,7 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
 
     def __exit__(self, *a):
         if self.proc:
@@ -135,10 +135,13 @@ class ClockSampler:
             if self.t:
                 self.t.join(timeout=2)
 
-    def summary(self):
+    def summary(self, t0=None, t1=None):
+        """Median SM clock and active throttle reasons of the samples taken
+        inside [t0, t1] (the timed region)."""
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        lines = [ln for (t, ln) in self.lines if (t0 is None or t >= t0) and (t1 is None or t <= t1)]
+        for ln in lines:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -240,7 +243,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--workload", default="bs8", choices=["bs8", "sf24"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
@@ -306,6 +309,8 @@ def main():
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     l0 = lds.launch_count()
     with ClockSampler(local) as clk:
+        time.sleep(0.5)                          # let the sampler start before the timed region
+        t_begin = time.time()
         with torch.cuda.stream(stream):
             for k in range(args.steps):
                 flush.fill_(float(k))            # evict L2 between steps (outside the events)
@@ -313,6 +318,8 @@ def main():
                 step()
                 evs[k][1].record(stream)
         torch.cuda.synchronize()
+        t_end = time.time()
+        time.sleep(0.1)
     launches = lds.launch_count() - l0
     lds._ext._sync_status(ds, s)
     times = [a.elapsed_time(b) for a, b in evs]
@@ -369,7 +376,7 @@ def main():
         "config": dict(cdesc, l2="flushed between steps (256 MB write outside the timed events)",
                        parallelism=f"replicas x{world}"),
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-        "clocks": clk.summary(),
+        "clocks": clk.summary(t_begin, t_end),
     }
     print(json.dumps(line), flush=True)
     if dist:
