@@ -167,6 +167,25 @@ int ld_gradient_dev(ld_descriptor *d, int n_rows, const int *row_centre,
                     const double *dE_ddesc, double *d_coords, double *desc_out,
                     const int *image, ld_stream stream);
 
+/* Descriptor + VJP pass that allocates no device memory (no counterpart in
+ * the reference; it serves callers that cannot call cudaMalloc while they
+ * evaluate forces, e.g. engines whose device memory is owned by their own
+ * pool or loops with a no-allocation rule).  Same arguments as
+ * ld_gradient_dev, except that it takes number_of_neighs (device, n_rows)
+ * instead of neigh_offsets: the row offsets, the prefix-sum work space and
+ * the status word live in a fixed 4 MiB array of the library's own device
+ * memory, held by every GPU that loads the library until the process exits.
+ * Limit: n_rows <= 262144 per call (larger requests return LD_ERR_CAPACITY).
+ * d_coords is accumulated into; the call waits for `stream` and returns any
+ * device-side status (LD_ERR_CAPACITY when a row exceeds max_neigh).  All
+ * calls share the array: calls that overlap on the GPU race on it. */
+int ld_gradient_counts_dev_noalloc(ld_descriptor *d, int n_rows, const int *row_centre,
+                                   const int *species, const int *neighbor_list,
+                                   const int *number_of_neighs, int max_neigh,
+                                   const double *coords, const double *dE_ddesc,
+                                   double *d_coords, double *desc_out, const int *image,
+                                   ld_stream stream);
+
 /* Wait for `stream` and return the first device-side error status raised by
  * this descriptor's kernels since the last call (then clear it). */
 int ld_sync_status(ld_descriptor *d, ld_stream stream);

@@ -32,7 +32,7 @@ INCLUDE = os.path.join(ROOT, "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                      "-I" + INCLUDE, "-I" + CSRC]
-CORE_SOURCES = ["ld_sf.cu", "ld_bs.cu", "ld_util.cu", "ld_core.cpp", "ld_neighbor.cpp"]
+CORE_SOURCES = ["ld_sf.cu", "ld_bs.cu", "ld_util.cu", "ld_core.cpp", "ld_neighbor.cpp", "ld_noalloc.cu"]
 HEADERS = [os.path.join(CSRC, "ld_internal.h"), os.path.join(INCLUDE, "libdescriptor_b200.h")]
 
 
