@@ -586,9 +586,35 @@ size_t bs_smem_bytes(const BSDev &p, int max_neigh, bool vjp) {
     return d * sizeof(double) + ints * sizeof(int);
 }
 
+template <int J>
+int bs2_launch_t(const BSDev &p, const RowArgs &a, cudaStream_t s);
+
+// twojmax-specialised path (ld_bs2*.cu): per-centre kernel + pair-parallel
+// gradient kernel; it needs a stream-ordered work space for Y, so the
+// no-allocation entry point and the Jacobian (row remapping) use the single
+// fused kernel below instead.
+static int bs2_dispatch(const BSDev &p, const RowArgs &a, cudaStream_t s) {
+    switch (p.J) {
+    case 0: return bs2_launch_t<0>(p, a, s);
+    case 1: return bs2_launch_t<1>(p, a, s);
+    case 2: return bs2_launch_t<2>(p, a, s);
+    case 3: return bs2_launch_t<3>(p, a, s);
+    case 4: return bs2_launch_t<4>(p, a, s);
+    case 5: return bs2_launch_t<5>(p, a, s);
+    case 6: return bs2_launch_t<6>(p, a, s);
+    case 7: return bs2_launch_t<7>(p, a, s);
+    case 8: return bs2_launch_t<8>(p, a, s);
+    case 9: return bs2_launch_t<9>(p, a, s);
+    case 10: return bs2_launch_t<10>(p, a, s);
+    }
+    return fail(LD_ERR_CAPACITY, "bispectrum: twojmax outside the compiled range");
+}
+
 int bs_launch(const BSDev &p, const RowArgs &a, cudaStream_t s) {
     if (a.n_rows <= 0) return LD_OK;
     const bool vjp = a.dE != nullptr;
+    if (!a.fused_only && a.row_list == nullptr && a.dc_stride == 0 && p.J <= kMaxTwoJ)
+        return bs2_dispatch(p, a, s);
     const int cap = a.max_neigh > 0 ? a.max_neigh : 1;
     const size_t smem = bs_smem_bytes(p, cap, vjp);
     if (smem > 227 * 1024)

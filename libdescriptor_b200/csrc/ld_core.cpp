@@ -265,10 +265,10 @@ struct BSTask {
 // Longest-processing-time assignment of Z-element tasks to kBSThreads
 // threads; tasks of one thread are stored contiguously, costliest first.
 static void lpt_schedule(const std::vector<BSTask> &tasks_in, const std::vector<std::array<int, 4>> &trip,
-                         const std::vector<int> &cgoff, std::vector<int> &toff, std::vector<int4> &packed) {
+                         const std::vector<int> &cgoff, std::vector<int> &toff, std::vector<int4> &packed,
+                         int nt = kBSThreads) {
     std::vector<BSTask> tasks = tasks_in;
     std::stable_sort(tasks.begin(), tasks.end(), [](const BSTask &a, const BSTask &b) { return a.cost > b.cost; });
-    const int nt = kBSThreads;
     std::vector<std::vector<BSTask>> bins(nt);
     using E = std::pair<long long, int>;
     std::priority_queue<E, std::vector<E>, std::greater<E>> heap;
@@ -443,13 +443,16 @@ static int build_bs_impl(ld_descriptor *d, double rfac0, int J, int style, doubl
         }
         return tasks;
     };
-    std::vector<int> toff_f, toff_v;
-    std::vector<int4> task_f, task_v;
+    std::vector<int> toff_f, toff_v, toff2_f, toff2_v;
+    std::vector<int4> task_f, task_v, task2_f, task2_v;
+    b.nt2 = 32 * bs2_warps(J);
     {
         auto tf = make_tasks(need_f, d->bs_inner_fwd);
         lpt_schedule(tf, trip, cgoff, toff_f, task_f);
+        lpt_schedule(tf, trip, cgoff, toff2_f, task2_f, b.nt2);
         auto tv = make_tasks(need_v, d->bs_inner_vjp);
         lpt_schedule(tv, trip, cgoff, toff_v, task_v);
+        lpt_schedule(tv, trip, cgoff, toff2_v, task2_v, b.nt2);
         d->bs_tasks_fwd = (int)tf.size();
         d->bs_tasks_vjp = (int)tv.size();
     }
@@ -476,6 +479,10 @@ static int build_bs_impl(ld_descriptor *d, double rfac0, int J, int style, doubl
     ar.add(task_f, &b.task_f);
     ar.add(toff_v, &b.toff_v);
     ar.add(task_v, &b.task_v);
+    ar.add(toff2_f, &b.toff2_f);
+    ar.add(task2_f, &b.task2_f);
+    ar.add(toff2_v, &b.toff2_v);
+    ar.add(task2_v, &b.task2_v);
     int rc = ar.upload(d->tables);
     if (rc) return rc;
     d->kind = LD_KIND_BISPECTRUM;

@@ -89,6 +89,12 @@ struct BSDev {
     const int4 *task_f = nullptr;
     const int *toff_v = nullptr;        // NT+1 (gradient: all needed triples)
     const int4 *task_v = nullptr;
+    // schedules of the twojmax-specialised per-centre kernel (nt2 threads)
+    int nt2 = 0;
+    const int *toff2_f = nullptr;
+    const int4 *task2_f = nullptr;
+    const int *toff2_v = nullptr;
+    const int4 *task2_v = nullptr;
 };
 
 constexpr int kBSThreads = 128;   // threads per bispectrum CTA (one centre)
@@ -112,7 +118,15 @@ struct RowArgs {
     long long dc_stride = 0;           // doubles between rows' gradients (0 = shared)
     const int *image = nullptr;
     int *status = nullptr;             // device error word
+    bool fused_only = false;           // gradient in one kernel, no work space (no allocation)
 };
+
+// warps of the twojmax-specialised per-centre bispectrum CTA (4..8)
+constexpr int bs2_warps(int J) {
+    return (36 + 32 / (J / 2 + 1) - 1) / (32 / (J / 2 + 1)) < 4   ? 4
+           : (36 + 32 / (J / 2 + 1) - 1) / (32 / (J / 2 + 1)) > 8 ? 8
+                                                                  : (36 + 32 / (J / 2 + 1) - 1) / (32 / (J / 2 + 1));
+}
 
 int sf_launch(const SFDev &p, const RowArgs &a, cudaStream_t s);
 int bs_launch(const BSDev &p, const RowArgs &a, cudaStream_t s);

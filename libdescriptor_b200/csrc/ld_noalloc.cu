@@ -98,6 +98,7 @@ extern "C" int ld_gradient_counts_dev_noalloc(ld_descriptor *d, int n_rows, cons
     a.dcoords = d_coords;
     a.image = image;
     a.status = status;
+    a.fused_only = true;   // single-kernel gradient: no stream-ordered work space
     rc = launch_rows(d, a, s);
     if (rc) return rc;
     int st = 0;
