@@ -193,6 +193,27 @@ static int build_sf(ld_descriptor *d, int ns, const double *cutoff, int n_types,
         if (x.t != y.t) return x.t < y.t;
         return x.eta < y.eta;
     });
+    std::vector<int> ec3;
+    {
+        int prev_t = -1;
+        double prev_eta = 0.0, base_eta = 0.0;
+        for (auto &q : three) {
+            int code = 0;
+            if (q.t == prev_t && q.eta == prev_eta) {
+                code = -1;
+            } else if (q.t != prev_t) {
+                base_eta = q.eta;   // smallest eta of the type group (sorted ascending)
+                code = 0;
+            } else if (base_eta > 0 && q.eta > 0) {
+                const double ratio = q.eta / base_eta;
+                const double k = std::floor(ratio + 0.5);
+                if (k >= 2 && k <= 256 && std::fabs(ratio - k) <= 1e-9 * ratio) code = (int)k;
+            }
+            ec3.push_back(code);
+            prev_t = q.t;
+            prev_eta = q.eta;
+        }
+    }
     for (auto &q : three) {
         o3.push_back(q.o);
         t3.push_back(q.t);
@@ -223,6 +244,7 @@ static int build_sf(ld_descriptor *d, int ns, const double *cutoff, int n_types,
     ar.add(l3, &s.l3);
     ar.add(e3, &s.e3);
     ar.add(zi3, &s.zi3);
+    ar.add(ec3, &s.ec3);
     int rc = ar.upload(d->tables);
     if (rc) return rc;
     d->kind = LD_KIND_SYMMETRY_FUNCTIONS;

@@ -62,6 +62,11 @@ struct SFDev {
     const double *l3 = nullptr;     // lambda
     const double *e3 = nullptr;     // eta
     const int *zi3 = nullptr;       // integer zeta (>=0) or -1
+    // exp reuse per three-body output: -1 same factor as the previous output,
+    // 0 evaluate exp(-eta S) (the first output of a type group sets the
+    // group base), k >= 2 the group base raised to the k-th power (eta is
+    // k times the group's smallest eta)
+    const int *ec3 = nullptr;
 };
 
 // ------------------------------------------------------------- bispectrum

@@ -46,7 +46,7 @@ __device__ __forceinline__ double warp_sum(double v) {
 }
 
 struct WarpSlice {
-    double *cx, *cy, *cz, *r, *rc, *fc, *dfc, *gx, *gy, *gz;
+    double *cx, *cy, *cz, *r, *ir, *rc, *fc, *dfc, *gx, *gy, *gz;
     int *spec, *idx, *inc;
 };
 
@@ -57,6 +57,7 @@ __device__ __forceinline__ WarpSlice slice(double *base, int cap, bool vjp) {
     s.cy = p; p += cap;
     s.cz = p; p += cap;
     s.r = p; p += cap;
+    s.ir = p; p += cap;
     s.rc = p; p += cap;
     s.fc = p; p += cap;
     if (vjp) {
@@ -75,7 +76,7 @@ __device__ __forceinline__ WarpSlice slice(double *base, int cap, bool vjp) {
 }
 
 template <bool VJP, int M2, int M3>
-__global__ void __launch_bounds__(kSFThreads)
+__global__ void __launch_bounds__(kSFThreads, VJP ? 3 : 4)
 sf_kernel(SFDev p, RowArgs a, int per_warp_doubles) {
     extern __shared__ double smem[];
     const int lane = threadIdx.x & 31;
@@ -118,6 +119,7 @@ sf_kernel(SFDev p, RowArgs a, int per_warp_doubles) {
             S.cy[jj] = y;
             S.cz[jj] = z;
             S.r[jj] = r;
+            S.ir[jj] = 1.0 / r;
             S.rc[jj] = rc;
             S.spec[jj] = js;
             S.idx[jj] = ok ? j : -1;
@@ -202,104 +204,131 @@ sf_kernel(SFDev p, RowArgs a, int per_warp_doubles) {
             }
             __syncwarp();
             while (jj < n - 1) {
-                if (S.inc[jj]) {
+                if (S.inc[jj] && S.inc[kk]) {
+                    // r_ik and its cutoff functions are the staged pair values of kk
+                    // (same coordinates, same species-pair cutoff as the reference's
+                    // per-triplet recomputation)
                     const int ks = S.spec[kk], js = S.spec[jj];
-                    const double rcik = p.rcut[is * p.ns + ks];
                     const double rcjk = p.rcut[js * p.ns + ks];
-                    const double xk = S.cx[kk], yk = S.cy[kk], zk = S.cz[kk];
-                    const double ikx = xk - cix, iky = yk - ciy, ikz = zk - ciz;
-                    const double jkx = xk - S.cx[jj], jky = yk - S.cy[jj], jkz = zk - S.cz[jj];
-                    const double riksq = ikx * ikx + iky * iky + ikz * ikz;
+                    const double jkx = S.cx[kk] - S.cx[jj], jky = S.cy[kk] - S.cy[jj], jkz = S.cz[kk] - S.cz[jj];
                     const double rjksq = jkx * jkx + jky * jky + jkz * jkz;
-                    const double b = sqrt(riksq);
                     const double d = sqrt(rjksq);
-                    if (!(b > rcik) && S.idx[kk] >= 0) {
-                        const double av = S.r[jj];
-                        const double asq = av * av, bsq = b * b, dsq = d * d;
-                        const double cth = (asq + bsq - dsq) / (2 * av * b);
-                        const double fa = S.fc[jj];
-                        const double fb = cutc(b, rcik);
-                        double fd, dfd = 0.0;
-                        {
-                            const double t = kPi * d / rcjk;
+                    const double av = S.r[jj], b = S.r[kk];
+                    const double ia = S.ir[jj], ib = S.ir[kk];
+                    const double asq = av * av, bsq = b * b, dsq = d * d;
+                    const double cth = (asq + bsq - dsq) * (0.5 * ia * ib);
+                    const double fa = S.fc[jj], fb = S.fc[kk];
+                    double fd = 0.0, dfd = 0.0;
+                    if (d < rcjk) {
+                        const double t = kPi * d / rcjk;
+                        if (VJP) {
                             double sn, cs;
                             sincos(t, &sn, &cs);
-                            fd = (d < rcjk) ? 0.5 * (cs + 1.0) : 0.0;
-                            if (VJP) dfd = (d < rcjk) ? -0.5 * sn * (kPi / rcjk) : 0.0;
+                            fd = 0.5 * (cs + 1.0);
+                            dfd = -0.5 * sn * (kPi / rcjk);
+                        } else {
+                            fd = 0.5 * (cos(t) + 1.0);
                         }
-                        const bool g4ok = !(d > rcjk);
-                        const double S4 = asq + bsq + dsq, S5 = asq + bsq;
-                        double A4 = 0, B4 = 0, C4 = 0, A5 = 0, B5 = 0, C5 = 0;
-                        double eprev = -1.0, E = 0.0;
-                        int tprev = 0;
+                    }
+                    const bool g4ok = !(d > rcjk);
+                    const double S4 = asq + bsq + dsq, S5 = asq + bsq;
+                    const double F4 = fa * fb * fd, F5 = fa * fb;
+                    double A4 = 0, B4 = 0, C4 = 0, A5 = 0, B5 = 0, C5 = 0;
+                    double E = 0.0, E0 = 0.0;
+                    int tprev = 0;
 #pragma unroll
-                        for (int q = 0; q < M3; ++q) {
-                            if (q < p.n3) {
-                                const int t = __ldg(p.t3 + q);
-                                if (t == 5 || g4ok) {
-                                    const double eta = __ldg(p.e3 + q);
-                                    if (eta != eprev || t != tprev) {
-                                        E = exp(-eta * (t == 4 ? S4 : S5));
-                                        eprev = eta;
-                                        tprev = t;
-                                    }
-                                    const double lam = __ldg(p.l3 + q);
-                                    const double base = 1.0 + lam * cth;
-                                    const int zi = __ldg(p.zi3 + q);
-                                    const double zeta = __ldg(p.z3 + q);
-                                    double cp = 0.0;
-                                    if (base > 0) cp = zi >= 0 ? ipow(base, zi) : pow(base, zeta);
-                                    const double P = __ldg(p.P3 + q);
-                                    const double v = (t == 4) ? P * cp * E * fa * fb * fd
-                                                              : P * cp * E * fa * fb;
-                                    acc3[q] += v;
-                                    if (VJP && base > 0) {
-                                        const double g = __ldg(dE + __ldg(p.o3 + q));
-                                        const double bq = g * P * E;
-                                        double dcp;
-                                        if (zi >= 0) dcp = zi > 0 ? zeta * ipow(base, zi - 1) : 0.0;
-                                        else dcp = zeta * pow(base, zeta - 1.0);
-                                        if (t == 4) {
-                                            A4 += bq * cp;
-                                            B4 += bq * cp * eta;
-                                            C4 += bq * dcp * lam;
+                    for (int q = 0; q < M3; ++q) {
+                        if (q < p.n3) {
+                            const int t = __ldg(p.t3 + q);
+                            const double eta = __ldg(p.e3 + q);
+                            const int ec = __ldg(p.ec3 + q);
+                            // exp(-eta S): once per distinct eta; integer multiples of the
+                            // group's smallest eta by powering (e^{kx} = (e^x)^k)
+                            if (t != tprev) {
+                                E0 = exp(-eta * (t == 4 ? S4 : S5));
+                                E = E0;
+                                tprev = t;
+                            } else if (ec == 0) {
+                                E = exp(-eta * (t == 4 ? S4 : S5));
+                            } else if (ec > 0) {
+                                double r = 1.0, x = E0;
+                                for (int k = ec; k > 0; k >>= 1) {
+                                    if (k & 1) r *= x;
+                                    x *= x;
+                                }
+                                E = r;
+                            }
+                            if (t == 5 || g4ok) {
+                                const double lam = __ldg(p.l3 + q);
+                                const double base = 1.0 + lam * cth;
+                                const int zi = __ldg(p.zi3 + q);
+                                double cp = 0.0, dcp = 0.0;
+                                if (base > 0) {
+                                    if (zi == 1) {
+                                        cp = base;
+                                        dcp = 1.0;
+                                    } else if (zi == 2) {
+                                        cp = base * base;
+                                        dcp = 2.0 * base;
+                                    } else if (zi == 4) {
+                                        const double b2 = base * base;
+                                        cp = b2 * b2;
+                                        dcp = 4.0 * b2 * base;
+                                    } else {
+                                        const double zeta = __ldg(p.z3 + q);
+                                        if (zi >= 0) {
+                                            cp = ipow(base, zi);
+                                            dcp = zi > 0 ? zeta * ipow(base, zi - 1) : 0.0;
                                         } else {
-                                            A5 += bq * cp;
-                                            B5 += bq * cp * eta;
-                                            C5 += bq * dcp * lam;
+                                            cp = pow(base, zeta);
+                                            dcp = zeta * pow(base, zeta - 1.0);
                                         }
+                                    }
+                                }
+                                const double P = __ldg(p.P3 + q);
+                                acc3[q] += P * cp * E * (t == 4 ? F4 : F5);
+                                if (VJP && base > 0) {
+                                    const double g = __ldg(dE + __ldg(p.o3 + q));
+                                    const double bq = g * P * E;
+                                    if (t == 4) {
+                                        A4 += bq * cp;
+                                        B4 += bq * cp * eta;
+                                        C4 += bq * dcp * lam;
+                                    } else {
+                                        A5 += bq * cp;
+                                        B5 += bq * cp * eta;
+                                        C5 += bq * dcp * lam;
                                     }
                                 }
                             }
                         }
-                        if (VJP) {
-                            const double dfa = S.dfc[jj];
-                            const double dfb = dcutc(b, rcik);
-                            const double dca = (asq - bsq + dsq) / (2 * asq * b);
-                            const double dcb = (bsq - asq + dsq) / (2 * av * bsq);
-                            const double dcd = -d / (av * b);
-                            const double F4 = fa * fb * fd, F5 = fa * fb;
-                            const double Ga = F4 * C4 * dca - 2.0 * av * F4 * B4 + dfa * fb * fd * A4 +
-                                              F5 * C5 * dca - 2.0 * av * F5 * B5 + dfa * fb * A5;
-                            const double Gb = F4 * C4 * dcb - 2.0 * b * F4 * B4 + fa * dfb * fd * A4 +
-                                              F5 * C5 * dcb - 2.0 * b * F5 * B5 + fa * dfb * A5;
-                            const double Gd = F4 * C4 * dcd - 2.0 * d * F4 * B4 + fa * fb * dfd * A4 +
-                                              F5 * C5 * dcd;
-                            const double ia = 1.0 / av, ib = 1.0 / b, id = d > 0 ? 1.0 / d : 0.0;
-                            const double ijx = (S.cx[jj] - cix) * ia, ijy = (S.cy[jj] - ciy) * ia,
-                                         ijz = (S.cz[jj] - ciz) * ia;
-                            const double ukx = ikx * ib, uky = iky * ib, ukz = ikz * ib;
-                            const double udx = jkx * id, udy = jky * id, udz = jkz * id;
-                            atomicAdd(&S.gx[jj], Ga * ijx - Gd * udx);
-                            atomicAdd(&S.gy[jj], Ga * ijy - Gd * udy);
-                            atomicAdd(&S.gz[jj], Ga * ijz - Gd * udz);
-                            atomicAdd(&S.gx[kk], Gb * ukx + Gd * udx);
-                            atomicAdd(&S.gy[kk], Gb * uky + Gd * udy);
-                            atomicAdd(&S.gz[kk], Gb * ukz + Gd * udz);
-                            gix -= Ga * ijx + Gb * ukx;
-                            giy -= Ga * ijy + Gb * uky;
-                            giz -= Ga * ijz + Gb * ukz;
-                        }
+                    }
+                    if (VJP) {
+                        const double dfa = S.dfc[jj], dfb = S.dfc[kk];
+                        const double dca = (asq - bsq + dsq) * (0.5 * ia * ia * ib);
+                        const double dcb = (bsq - asq + dsq) * (0.5 * ia * ib * ib);
+                        const double dcd = -d * ia * ib;
+                        const double Ga = F4 * C4 * dca - 2.0 * av * F4 * B4 + dfa * fb * fd * A4 +
+                                          F5 * C5 * dca - 2.0 * av * F5 * B5 + dfa * fb * A5;
+                        const double Gb = F4 * C4 * dcb - 2.0 * b * F4 * B4 + fa * dfb * fd * A4 +
+                                          F5 * C5 * dcb - 2.0 * b * F5 * B5 + fa * dfb * A5;
+                        const double Gd = F4 * C4 * dcd - 2.0 * d * F4 * B4 + fa * fb * dfd * A4 +
+                                          F5 * C5 * dcd;
+                        const double id = d > 0 ? 1.0 / d : 0.0;
+                        const double ijx = (S.cx[jj] - cix) * ia, ijy = (S.cy[jj] - ciy) * ia,
+                                     ijz = (S.cz[jj] - ciz) * ia;
+                        const double ukx = (S.cx[kk] - cix) * ib, uky = (S.cy[kk] - ciy) * ib,
+                                     ukz = (S.cz[kk] - ciz) * ib;
+                        const double udx = jkx * id, udy = jky * id, udz = jkz * id;
+                        atomicAdd(&S.gx[jj], Ga * ijx - Gd * udx);
+                        atomicAdd(&S.gy[jj], Ga * ijy - Gd * udy);
+                        atomicAdd(&S.gz[jj], Ga * ijz - Gd * udz);
+                        atomicAdd(&S.gx[kk], Gb * ukx + Gd * udx);
+                        atomicAdd(&S.gy[kk], Gb * uky + Gd * udy);
+                        atomicAdd(&S.gz[kk], Gb * ukz + Gd * udz);
+                        gix -= Ga * ijx + Gb * ukx;
+                        giy -= Ga * ijy + Gb * uky;
+                        giz -= Ga * ijz + Gb * ukz;
                     }
                 }
                 // advance 32 triplets along the flattened upper triangle
@@ -345,7 +374,7 @@ sf_kernel(SFDev p, RowArgs a, int per_warp_doubles) {
 template <bool VJP, int M2, int M3>
 int launch_t(const SFDev &p, const RowArgs &a, cudaStream_t s) {
     const int cap = a.max_neigh > 0 ? a.max_neigh : 1;
-    const int ndbl = cap * (VJP ? 10 : 6);
+    const int ndbl = cap * (VJP ? 11 : 7);
     const int per_warp = ndbl + (3 * cap + 1) / 2 + 2;  // doubles (ints packed after)
     const size_t per_warp_bytes = (size_t)per_warp * sizeof(double);
     int nw = 4;
