@@ -3,16 +3,26 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
 
-A step is one fused descriptor + force-VJP pass (FP64) over one batch of
-synthetic input, with inputs resident in HBM.  Workloads (seeded, synthetic):
+Workloads (seeded synthetic inputs; the reference names no dataset):
 
-  bs8   8192-atom two-species random packing (0.05 A^-3, d_min 2 A, rc 5 A),
-        bispectrum 2J=8 (55 components), desc + VJP vs N(0,1) upstream
-  sf24  4096-atom Si diamond 8x8x8 (jitter 0.1 A), 24-d symmetry functions,
-        desc + VJP
+  serve     (default) the served mixed stream: periodic two-species random
+            packings (0.05 A^-3, d_min 2 A, rc 5 A) with log-uniform atom
+            counts in [16, 32768], 70% 24-d symmetry functions / 30%
+            bispectrum 2J=8, desc + VJP vs N(0,1) upstream, Poisson arrivals.
+            A step is 200 requests.  value: the batched resident pass over
+            each step's requests (inputs in HBM); e2e: the continuous-batching
+            server, host arrays in and out, at the top arrival rate, beside
+            the plain per-call path (one compute_and_gradient per request) on
+            the same stream; p50/p99 latency at 1k / 10k / 50k requests/s.
+  batch512  512 strained, jittered Si diamond supercells n_i ~ U{1..6}, each
+            with 24-d symmetry functions and bispectrum 2J=6, desc + VJP: one
+            persistent launch per descriptor under a CUDA graph (autotuned
+            launch shape) vs the per-configuration launch loop.
+  bs8       8192-atom two-species packing, bispectrum 2J=8, desc + VJP
+  sf24      4096-atom Si diamond 8x8x8 (jitter 0.1 A), 24-d symmetry functions
 
 Multi-GPU (torchrun): replicas only -- every rank runs its own independent
-batch (the path has no exchange step); value = all ranks' atoms / max time.
+work (the path has no exchange step); value = all ranks' atoms / max time.
 """
 from __future__ import annotations
 
@@ -30,26 +40,39 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "desc+VJP atoms/s"
+METRIC = "desc+VJP atoms/s, 1 B200: served batch vs plain call; p50/p99 ms @≤1e-10 rel"
+RATES = (1000.0, 10000.0, 50000.0)
+REQ_PER_STEP = 200
+MIX = {"sf": 0.7, "bs": 0.3}
 
 
-# --------------------------------------------------------------- workloads
+# --------------------------------------------------------------- specs
+def sf24_spec(species):
+    from libdescriptor_b200 import workloads as W
+
+    t, sz, p = W.sf24_params()
+    return dict(kind="sf", types=t, sizes=sz, params=p, cutoff=5.0, species=list(species))
+
+
+def bs_spec(J, species, weights):
+    return dict(kind="bs", rfac0=0.99363, twojmax=J, style=3, rmin0=0.0, switch_flag=1, bzero_flag=0, cutoff=5.0,
+                species=list(species), weights=list(weights))
+
+
 def make_workload(name: str, seed: int):
     from libdescriptor_b200 import workloads as W
 
     if name == "bs8":
         x, cell, sp = W.random_packing(8192, density=0.05, dmin=2.0, n_species=2, seed=seed)
         cfg = W.prepare(x, cell, sp, 5.0)
-        spec = dict(kind="bs", rfac0=0.99363, twojmax=8, style=3, rmin0=0.0, switch_flag=1, bzero_flag=0,
-                    cutoff=5.0, species=["A", "B"], weights=[1.0, 0.5])
+        spec = bs_spec(8, ["A", "B"], [1.0, 0.5])
         desc = {"workload": "bispectrum_2J8_random_packing_8192", "atoms": 8192, "twojmax": 8, "width": 55,
                 "species": 2, "density": 0.05, "cutoff": 5.0, "box_side": float(cell[0, 0])}
     elif name == "sf24":
         x, cell = W.diamond_cell(8, 8, 8, jitter=0.1, seed=seed)
         sp = np.zeros(len(x), np.int32)
         cfg = W.prepare(x, cell, sp, 5.0)
-        t, sz, p = W.sf24_params()
-        spec = dict(kind="sf", types=t, sizes=sz, params=p, cutoff=5.0, species=["Si"])
+        spec = sf24_spec(["Si"])
         desc = {"workload": "symmetry_functions_24_diamond_8x8x8", "atoms": 4096, "width": 24, "cutoff": 5.0}
     else:
         raise SystemExit(f"unknown workload {name}")
@@ -81,6 +104,7 @@ def make_oracle(spec):
 
 
 def algorithmic_flops(spec, cfg, weights):
+    """Algorithmic FP64 flops of one desc+VJP pass over cfg's centres."""
     from libdescriptor_b200 import flops as F
 
     if spec["kind"] == "bs":
@@ -90,6 +114,8 @@ def algorithmic_flops(spec, cfg, weights):
         return per * cfg.n_atoms + nb * n_in
     # symmetry functions (8 g2 + 16 g4 rows (zeta, lambda, eta)): triplets
     # counted exactly from the neighbour lists
+    if cfg.n_atoms == 0:
+        return 0.0
     trip = float(np.sum(cfg.counts * (cfg.counts - 1) / 2.0))
     n_eta = len(set(np.asarray(spec["params"])[16 + 2::3]))
     return F.sf_flops_per_atom(float(cfg.counts.mean()), 8, 16, n_eta, True,
@@ -135,12 +161,12 @@ class ClockSampler:
             if self.t:
                 self.t.join(timeout=2)
 
-    def summary(self, t0=None, t1=None):
+    def summary(self, windows):
         """Median SM clock and active throttle reasons of the samples taken
-        inside [t0, t1] (the timed region)."""
+        inside the timed windows [(t0, t1), ...]."""
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        lines = [ln for (t, ln) in self.lines if (t0 is None or t >= t0) and (t1 is None or t <= t1)]
+        lines = [ln for (t, ln) in self.lines if any(a <= t <= b for a, b in windows)]
         for ln in lines:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
@@ -160,29 +186,35 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------- CPU legs
-def cpu_desc_vjp_rate(spec, cfg, budget_s=12.0, threads=None):
-    """Oracle desc+VJP atoms/s on a bounded sample of the same workload."""
+def cpu_rate(spec, cfgs, budget_s=10.0, threads=None):
+    """Oracle desc+VJP atoms/s (all host threads) on a bounded sample: whole
+    configurations of ``cfgs`` in order until about budget_s of work."""
     ora = make_oracle(spec)
     threads = threads or os.cpu_count() or 1
     rng = np.random.default_rng(7)
 
-    def run(nrows):
-        rows = np.arange(nrows, dtype=np.int32)
+    def run(cfg, nrows):
         dE = rng.normal(size=(nrows, ora.width))
         t0 = time.perf_counter()
         ora.run(np.array([nrows], np.int32), cfg.species, cfg.nbl, cfg.counts[:nrows], cfg.coords, dE=dE,
                 n_configs=1, config_ptr=np.array([0], np.int32), n_threads=threads)
-        del rows
         return time.perf_counter() - t0
 
-    n0 = min(cfg.n_atoms, max(threads, 16))
-    t0 = run(n0)
-    n1 = int(min(cfg.n_atoms, max(n0, n0 * budget_s / max(t0, 1e-6))))
-    t1 = run(n1)
-    return n1 / t1, n1, threads
+    atoms, secs = 0, 0.0
+    for cfg in cfgs:
+        n = cfg.n_atoms
+        if secs > 0 and atoms > 0:
+            # cap the last configuration so the sample stays near the budget
+            rate = atoms / secs
+            n = int(min(n, max(16, (budget_s - secs) * rate)))
+        secs += run(cfg, n)
+        atoms += n
+        if secs >= budget_s:
+            break
+    return atoms / secs, atoms, threads
 
 
-def reference_forward_rate(spec, cfg, budget_s=5.0, threads=None):
+def reference_forward_rate(spec, cfg, budget_s=4.0, threads=None):
     from oracle import Reference, ReferenceDescriptor
 
     if not Reference.available():
@@ -208,69 +240,309 @@ def reference_forward_rate(spec, cfg, budget_s=5.0, threads=None):
     return n1 / run(n1)
 
 
-def run_reference(args):
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
-        return
-    cfg, spec, cdesc = make_workload(args.workload, seed=1)
+def mix_cpu_rate(specs, requests, budget_s):
+    """CPU desc+VJP atoms/s of the request mix: each lane's rate on a sample
+    of its own requests, combined by the lanes' atom shares."""
     threads = os.cpu_count() or 1
-    rates = []
-    sample = None
-    for _ in range(args.warmup):
-        cpu_desc_vjp_rate(spec, cfg, budget_s=2.0, threads=threads)
-    for _ in range(args.steps):
-        r, n, _ = cpu_desc_vjp_rate(spec, cfg, budget_s=6.0, threads=threads)
-        rates.append(r)
-        sample = n
-    value = statistics.mean(rates)
-    fwd = reference_forward_rate(spec, cfg, threads=threads)
-    line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "atoms/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sample / value,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": cdesc,
-        "cpu_baseline": {"value": value, "unit": "atoms/s", "cores": threads, "kind": "port",
-                         "sample": f"{sample} centres of the workload per step, desc+VJP by the oracle's "
-                                   f"analytic adjoint (the reference's Enzyme gradient cannot be built "
-                                   f"offline); reference C++ forward alone: "
-                                   f"{fwd if fwd is None else round(fwd, 1)} atoms/s"},
-        "e2e": {"value": value, "unit": "atoms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
-    print(json.dumps(line), flush=True)
+    atoms = {k: sum(r.n_atoms for r in requests if r.lane == k) for k in specs}
+    tot = sum(atoms.values())
+    secs_per_atom, samples = 0.0, []
+    for k, spec in specs.items():
+        cfgs = [r.cfg for r in requests if r.lane == k]
+        if not cfgs:
+            continue
+        r, n, _ = cpu_rate(spec, cfgs, budget_s=budget_s * atoms[k] / tot, threads=threads)
+        secs_per_atom += (atoms[k] / tot) / r
+        samples.append(f"{n} {k} centres")
+    return 1.0 / secs_per_atom, ", ".join(samples), threads
 
 
-# ------------------------------------------------------------------- GPU
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--workload", default="bs8", choices=["bs8", "sf24"])
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    args = ap.parse_args()
-    args.warmup = max(args.warmup, 3)
-    if args.impl == "reference":
-        run_reference(args)
-        return
+# ------------------------------------------------------------------ serve
+def serve_setup(seed=1, n_pool=32):
+    from libdescriptor_b200 import serving as S
 
-    import torch
+    pool = S.packing_pool(n_pool, n_min=16, n_max=32768, seed=seed)
+    specs = {"sf": sf24_spec(["A", "B"]), "bs": bs_spec(8, ["A", "B"], [1.0, 0.5])}
+    return pool, specs
 
-    import libdescriptor_b200 as lds
+
+def tag_requests(reqs, pool):
+    """Attach each request's pool configuration (for the resident pass)."""
+    by_id = {id(c.coords): c for c in pool}
+    for r in reqs:
+        r.cfg = by_id[id(r.coords)]
+    return reqs
+
+
+def run_serve(args, torch, lds, dev, world, rank, local, dist):
+    from libdescriptor_b200 import batch as B
     from libdescriptor_b200 import flops as F
+    from libdescriptor_b200 import serving as S
+    from libdescriptor_b200 import workloads as W
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
+    pool, specs = serve_setup(seed=1 + rank)
+    kinds = {k: make_descriptor(s) for k, s in specs.items()}
+    widths = {k: int(v.width) for k, v in kinds.items()}
+    K = args.steps
+    nreq = K * REQ_PER_STEP
+    reqs = tag_requests(S.make_requests(pool, nreq, widths, MIX, seed=11 + rank), pool)
+    # at most 10 distinct steps are kept resident; longer runs cycle over them
+    steps = [reqs[i * REQ_PER_STEP:(i + 1) * REQ_PER_STEP] for i in range(min(K, 10))]
 
-        import torch.distributed as dist
+    peak = lds.measure_fp64_peak(4096)
+    weights = F.measure_weights(peak)
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    dev = torch.device("cuda", local)
+    # ---- value: one batched resident pass per lane over each step's requests
+    passes = []
+    for st in steps:
+        per = {}
+        for k in kinds:
+            cfgs = [r.cfg for r in st if r.lane == k]
+            if not cfgs:
+                continue
+            b = W.concat(cfgs)
+            db = B.DeviceBatch.from_batch(b, kinds[k], device=dev)
+            dE = torch.randn(db.n_rows, widths[k], dtype=torch.float64, device=dev)
+            per[k] = (B.BatchedPass(kinds[k], db, dE), sum(algorithmic_flops(specs[k], c, weights) for c in cfgs))
+        passes.append(per)
+    stream = torch.cuda.Stream(device=dev)
+    for per in passes:
+        for ps, _ in per.values():
+            ps.stream = stream
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            for ps, _ in passes[0].values():
+                ps.run()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    evs = {k: [] for k in kinds}
+    l0 = lds.launch_count()
+    windows = []
+    with ClockSampler(local) as clk:
+        time.sleep(0.3)
+        t_a = time.time()
+        with torch.cuda.stream(stream):
+            for i in range(K):
+                for k, (ps, _) in passes[i % len(passes)].items():
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    ps.run()
+                    e1.record(stream)
+                    evs[k].append((e0, e1))
+        torch.cuda.synchronize()
+        windows.append((t_a, time.time()))
+        launches = lds.launch_count() - l0
+        for ps, _ in passes[0].values():
+            ps.sync_status()
+        ms = {k: sum(a.elapsed_time(b) for a, b in v) for k, v in evs.items()}
+        tot_ms = sum(ms.values())
+        if dist:
+            t = torch.tensor([tot_ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            tot_ms = float(t.item())
+        step_atoms = [sum(r.n_atoms for r in st) for st in steps]
+        atoms_timed = sum(step_atoms[i % len(steps)] for i in range(K))
+        atoms_total = sum(r.n_atoms for r in reqs)
+        value = world * atoms_timed / (tot_ms * 1e-3)
+        flops_timed = {k: sum(per[k][1] for i in range(K) for per in [passes[i % len(passes)]] if k in per)
+                       for k in kinds}
+        del passes
+        torch.cuda.empty_cache()
+
+        # ---- e2e: the server at every rate, and the plain per-call path
+        eng = S.ServingEngine(kinds, budget_bytes=40 << 30, shares={"sf": 0.45, "bs": 0.55}, device=dev)
+        warm = tag_requests(S.make_requests(pool, 64, widths, MIX, seed=99), pool)
+        eng.serve(warm, None)
+        sweep = []
+        h2d_bytes = sum(r.coords.nbytes + r.species.nbytes + r.image.nbytes + r.nbl.nbytes + r.counts.nbytes
+                        + r.dE.nbytes + 12 * r.n_atoms for r in reqs)
+        d2h_bytes = sum(8 * r.n_atoms * (widths[r.lane] + 3) for r in reqs)
+        served = None
+        for rate in sorted(RATES):
+            rs = tag_requests(S.make_requests(pool, nreq, widths, MIX, seed=11 + rank), pool)
+            eng.sched.batch_rows, eng.sched.batch_reqs, eng.sched.n_batches = [], [], 0
+            eng.launches = 0
+            t_b = time.time()
+            res = eng.serve(rs, S.poisson_arrivals(nreq, rate, seed=21))
+            windows.append((t_b, time.time()))
+            res["rate_per_s"] = rate
+            sweep.append({k: (round(v, 4) if isinstance(v, float) else v) for k, v in res.items()})
+            served = res
+        del eng
+        torch.cuda.empty_cache()
+        rs = S.make_requests(pool, nreq, widths, MIX, seed=11 + rank)
+        plain = S.serve_plain(kinds, rs, S.poisson_arrivals(nreq, max(RATES), seed=21))
+    if rank != 0:
+        return None
+    bs_flops, sf_flops = flops_timed["bs"], flops_timed["sf"]
+    ach_bs = bs_flops / (ms["bs"] * 1e-3) / 1e12 if ms.get("bs") else 0.0
+    ach_sf = sf_flops / (ms["sf"] * 1e-3) / 1e12 if ms.get("sf") else 0.0
+    roof = {"bound": "fp64", "achieved": ach_bs, "peak": peak, "unit": "TFLOP/s", "frac": ach_bs / peak,
+            "traffic": None, "kernel": "bsA_kernel<8,1> + bsB_kernel<8> (bispectrum 2J=8 lane of the batched pass)",
+            "flops_per_step": bs_flops / K, "share_of_pass_time": ms.get("bs", 0.0) / tot_ms,
+            "peak_source": "bench.py FP64 FMA probe (ld_measure_fp64_peak), same run; MEASURED_PEAKS.json has no "
+                           "FP64 figure",
+            "call_weights_flops": {k: round(v, 1) for k, v in weights.items()},
+            "sf_lane": {"achieved": ach_sf, "frac": ach_sf / peak, "kernel": "sf_kernel<1,32,32>",
+                        "share_of_pass_time": ms.get("sf", 0.0) / tot_ms}}
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        r, sample, thr = mix_cpu_rate(specs, reqs[:REQ_PER_STEP], budget_s=12.0)
+        cpu = {"value": r, "unit": "atoms/s", "cores": thr, "kind": "port",
+               "sample": f"{sample} of the first step's requests (whole configurations in order), desc+VJP by "
+                         f"the oracle's analytic adjoint on all host threads, combined by the mix's atom shares"}
+    e2e = {"value": world * served["atoms_per_s"], "unit": "atoms/s",
+           "h2d_bytes_per_step": int(h2d_bytes / K), "d2h_bytes_per_step": int(d2h_bytes / K),
+           "api": "libdescriptor_b200.serving.ServingEngine.serve (host numpy requests in, host results out), "
+                  f"Poisson arrivals at {int(max(RATES))}/s",
+           "p50_ms": served["p50_ms"], "p99_ms": served["p99_ms"],
+           "plain_call": {"value": world * plain["atoms_per_s"], "p50_ms": plain["p50_ms"], "p99_ms": plain["p99_ms"],
+                          "api": "libdescriptor_b200.compute_and_gradient per request + host fold"},
+           "served_over_plain": served["atoms_per_s"] / plain["atoms_per_s"],
+           "rate_sweep": sweep}
+    cdesc = {"workload": "served_mixed_stream_sf24_70_bs2J8_30", "requests": nreq, "requests_per_step": REQ_PER_STEP,
+             "atoms": int(atoms_total), "pool_configurations": len(pool), "atoms_log_uniform": [16, 32768],
+             "density": 0.05, "d_min": 2.0, "cutoff": 5.0, "mix": MIX, "hbm_budget_gb": 40,
+             "l2": "inputs of every step (>= 100 MB per lane pass) exceed the 126 MB L2 footprint reuse; no flush",
+             "value": "batched resident pass (one launch per lane per step, inputs in HBM)",
+             "parallelism": f"replicas x{world}"}
+    return {
+        "metric": METRIC, "value": value, "unit": "atoms/s", "n_gpus": world, "steps": K, "warmup": args.warmup,
+        "ms_per_step": tot_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded packings, no dataset)", "config": cdesc, "roofline": roof,
+        "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk.summary(windows),
+        "p50_ms": served["p50_ms"], "p99_ms": served["p99_ms"],
+    }
+
+
+# --------------------------------------------------------------- batch512
+def run_batch512(args, torch, lds, dev, world, rank, local, dist):
+    from libdescriptor_b200 import batch as B
+    from libdescriptor_b200 import flops as F
+    from libdescriptor_b200 import serving as S
+    from libdescriptor_b200 import tuner
+    from libdescriptor_b200 import workloads as W
+
+    cfgs = B.diamond_batch(512, seed=1 + rank)
+    b = W.concat(cfgs)
+    specs = {"sf24": sf24_spec(["Si"]), "bs6": bs_spec(6, ["Si"], [1.0])}
+    kinds = {k: make_descriptor(s) for k, s in specs.items()}
+    peak = lds.measure_fp64_peak(4096)
+    weights = F.measure_weights(peak)
+    tu = tuner.Autotuner(cache_path=os.path.join(ROOT, "gpurun_out", "tuning_cache.json")
+                         if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else None)
+    passes, chosen, loop_ms = {}, {}, {}
+    stream = torch.cuda.Stream(device=dev)
+    for k, kind in kinds.items():
+        db = B.DeviceBatch.from_batch(b, kind, device=dev)
+        dE = torch.randn(db.n_rows, int(kind.width), dtype=torch.float64, device=dev)
+        ps = B.BatchedPass(kind, db, dE, stream=stream)
+        chosen[k] = tu.tune(ps, k, 0 if k.startswith("sf") else 1)
+        # the per-configuration launch loop (same arena, one call per cell)
+        ps.run_per_config()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ps.run_per_config()
+        e1.record(stream)
+        e1.synchronize()
+        loop_ms[k] = e0.elapsed_time(e1)
+        ps.capture()
+        passes[k] = ps
+    n_rows = b.n_rows
+    for _ in range(args.warmup):
+        for ps in passes.values():
+            ps.replay()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    evs = {k: [] for k in passes}
+    l0 = lds.launch_count()
+    with ClockSampler(local) as clk:
+        time.sleep(0.3)
+        t_a = time.time()
+        with torch.cuda.stream(stream):
+            for _ in range(args.steps):
+                for k, ps in passes.items():
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    ps.replay()
+                    e1.record(stream)
+                    evs[k].append((e0, e1))
+        torch.cuda.synchronize()
+        t_b = time.time()
+    for ps in passes.values():
+        ps.sync_status()
+    # graph replays: count kernels per captured pass
+    launches = sum(ps.launches_per_pass for ps in passes.values()) * args.steps
+    ms = {k: sum(a.elapsed_time(b_) for a, b_ in v) / args.steps for k, v in evs.items()}
+    step_ms = sum(ms.values())
+    if dist:
+        t = torch.tensor([step_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        step_ms = float(t.item())
+    value = world * n_rows / (step_ms * 1e-3)
+    # e2e: the same 512 cells x 2 descriptors as requests to the server, host in/out
+    reqs = []
+    rng = np.random.default_rng(5)
+    for i, c in enumerate(cfgs):
+        for k, kind in kinds.items():
+            reqs.append(S.Request(len(reqs), k, c.n_atoms, c.coords, c.species, c.image, c.counts, c.nbl,
+                                  rng.normal(size=(c.n_atoms, int(kind.width)))))
+    eng = S.ServingEngine(kinds, budget_bytes=8 << 30, device=dev, tuning=chosen)
+    eng.serve(reqs[:64], None)
+    for r in reqs:
+        r.slots = None
+    t0 = time.perf_counter()
+    st = eng.serve(reqs, None)
+    e2e_s = time.perf_counter() - t0
+    if rank != 0:
+        return None
+    flop = {k: sum(algorithmic_flops(specs[k], c, weights) for c in cfgs) for k in specs}
+    dom = max(ms, key=ms.get)
+    ach = flop[dom] / (ms[dom] * 1e-3) / 1e12
+    roof = {"bound": "fp64", "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak, "traffic": None,
+            "kernel": f"{dom} batched pass", "flops_per_step": flop[dom],
+            "share_of_step_time": ms[dom] / step_ms,
+            "peak_source": "bench.py FP64 FMA probe (ld_measure_fp64_peak), same run"}
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        secs = 0.0
+        samples = []
+        for k, spec in specs.items():
+            r, n, thr = cpu_rate(spec, cfgs, budget_s=6.0)
+            secs += 1.0 / r
+            samples.append(f"{n} centres ({k})")
+        cpu = {"value": 1.0 / secs, "unit": "atoms/s", "cores": os.cpu_count() or 1, "kind": "port",
+               "sample": ", ".join(samples) + " of the cells in order; every atom gets both descriptors, desc+VJP "
+                                               "by the oracle on all host threads"}
+    h2d = sum(r.coords.nbytes + r.species.nbytes + r.image.nbytes + r.nbl.nbytes + r.counts.nbytes + r.dE.nbytes
+              + 12 * r.n_atoms for r in reqs)
+    d2h = sum(8 * r.n_atoms * (int(kinds[r.lane].width) + 3) for r in reqs)
+    cdesc = {"workload": "batched_512_diamond_cells_sf24_and_bs2J6", "cells": 512, "atoms": int(n_rows),
+             "n_cells_per_axis": "U{1..6}", "strain": 0.03, "jitter": 0.1, "cutoff": 5.0,
+             "tuned_launch_shape": chosen,
+             "per_config_loop_ms": loop_ms, "graph_pass_ms": ms,
+             "per_config_loop_atoms_per_s": world * n_rows / (sum(loop_ms.values()) * 1e-3),
+             "l2": "inputs exceed L2 (549,722 coordinate rows, ~20 MB neighbour lists, 100+ MB dL/d(desc)); no flush",
+             "parallelism": f"replicas x{world}"}
+    return {
+        "metric": METRIC, "value": value, "unit": "atoms/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded cells, no dataset)", "config": cdesc,
+        "roofline": roof, "cpu_baseline": cpu,
+        "e2e": {"value": world * n_rows / e2e_s, "unit": "atoms/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * e2e_s,
+                "api": "ServingEngine.serve of the 1024 (cell, descriptor) requests, host numpy in/out",
+                "batches": st["batches"]},
+        "gpu_launches": int(launches), "clocks": clk.summary([(t_a, t_b)]),
+    }
+
+
+# ----------------------------------------------------------- single cell
+def run_single(args, torch, lds, dev, world, rank, local, dist):
+    from libdescriptor_b200 import flops as F
 
     cfg, spec, cdesc = make_workload(args.workload, seed=1 + rank)
     ds = make_descriptor(spec)
@@ -309,7 +581,7 @@ def main():
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     l0 = lds.launch_count()
     with ClockSampler(local) as clk:
-        time.sleep(0.5)                          # let the sampler start before the timed region
+        time.sleep(0.5)
         t_begin = time.time()
         with torch.cuda.stream(stream):
             for k in range(args.steps):
@@ -322,63 +594,158 @@ def main():
         time.sleep(0.1)
     launches = lds.launch_count() - l0
     lds._ext._sync_status(ds, s)
-    times = [a.elapsed_time(b) for a, b in evs]
-    tot_ms = float(sum(times))
+    tot_ms = float(sum(a.elapsed_time(b) for a, b in evs))
     if dist:
         t = torch.tensor([tot_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         tot_ms = float(t.item())
     ms_per_step = tot_ms / args.steps
     value = world * n / (ms_per_step * 1e-3)
-
-    # ---- end to end through the public API: host buffers in, host results out
-    e2e = None
-    if rank == 0 or world > 1:
-        for _ in range(2):
-            lds.compute_and_gradient(ds, n, cfg.species, cfg.nbl, cfg.counts, cfg.coords, dE_h)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        ke = max(3, min(args.steps, 10))
-        for _ in range(ke):
-            lds.compute_and_gradient(ds, n, cfg.species, cfg.nbl, cfg.counts, cfg.coords, dE_h)
-        e2e_s = (time.perf_counter() - t0) / ke
-        h2d = cfg.species.nbytes + cfg.nbl.nbytes + cfg.counts.nbytes + cfg.coords.nbytes + dE_h.nbytes + 8 * (n + 1)
-        d2h = 8 * n * W + 8 * 3 * cfg.n_total
-        e2e = {"value": world * n / e2e_s, "unit": "atoms/s", "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * e2e_s,
-               "api": "libdescriptor_b200.compute_and_gradient (host numpy in/out, one fused pass)"}
-
+    for _ in range(2):
+        lds.compute_and_gradient(ds, n, cfg.species, cfg.nbl, cfg.counts, cfg.coords, dE_h)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ke = max(3, min(args.steps, 10))
+    for _ in range(ke):
+        lds.compute_and_gradient(ds, n, cfg.species, cfg.nbl, cfg.counts, cfg.coords, dE_h)
+    e2e_s = (time.perf_counter() - t0) / ke
+    h2d = cfg.species.nbytes + cfg.nbl.nbytes + cfg.counts.nbytes + cfg.coords.nbytes + dE_h.nbytes + 8 * (n + 1)
+    d2h = 8 * n * W + 8 * 3 * cfg.n_total
+    e2e = {"value": world * n / e2e_s, "unit": "atoms/s", "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * e2e_s,
+           "api": "libdescriptor_b200.compute_and_gradient (host numpy in/out, one fused pass)"}
     if rank != 0:
-        if dist:
-            dist.barrier()
-            dist.destroy_process_group()
-        return
-
+        return None
     flop = algorithmic_flops(spec, cfg, weights)
     achieved = flop / (ms_per_step * 1e-3) / 1e12
     roof = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-            "traffic": None, "kernel": "bs_kernel<VJP>" if spec["kind"] == "bs" else "sf_kernel<VJP>",
+            "traffic": None, "kernel": "bsA_kernel<8,1> + bsB_kernel<8>" if spec["kind"] == "bs" else "sf_kernel<1,32,32>",
             "flops_per_step": flop, "peak_source": "bench.py FP64 FMA probe (ld_measure_fp64_peak), same run",
             "call_weights_flops": {k: round(v, 1) for k, v in weights.items()},
             "hbm_bytes_per_step_algorithmic": int(cfg.coords.nbytes + cfg.nbl.nbytes + 8 * n * W * 2
                                                   + 24 * cfg.n_total)}
     cpu = None
     if not args.no_cpu_baseline and world == 1:
-        r, sample, thr = cpu_desc_vjp_rate(spec, cfg, budget_s=10.0)
+        r, sample, thr = cpu_rate(spec, [cfg], budget_s=10.0)
         fwd = reference_forward_rate(spec, cfg, budget_s=4.0)
         cpu = {"value": r, "unit": "atoms/s", "cores": thr, "kind": "port",
                "sample": f"{sample} of {n} centres, desc+VJP by the oracle's analytic adjoint on all host "
                          f"threads; reference C++ forward alone: {None if fwd is None else round(fwd, 1)} atoms/s"}
-    line = {
+    return {
         "metric": METRIC, "value": value, "unit": "atoms/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, no dataset)",
         "config": dict(cdesc, l2="flushed between steps (256 MB write outside the timed events)",
                        parallelism=f"replicas x{world}"),
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-        "clocks": clk.summary(t_begin, t_end),
+        "clocks": clk.summary([(t_begin, t_end)]),
+    }
+
+
+# -------------------------------------------------------- reference arm
+def run_reference(args):
+    """The reference-side CPU path of the same workload: the oracle's
+    desc+VJP (a restatement of the reference's algorithm; its Enzyme
+    gradient cannot be built offline) on all host threads."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    rates, sample = [], None
+    if args.workload == "serve":
+        from libdescriptor_b200 import serving as S
+
+        pool, specs = serve_setup(seed=1)
+        widths = {"sf": 24, "bs": 55}
+        reqs = tag_requests(S.make_requests(pool, REQ_PER_STEP, widths, MIX, seed=11), pool)
+
+        def one(budget):
+            return mix_cpu_rate(specs, reqs, budget)
+
+        cdesc = {"workload": "served_mixed_stream_sf24_70_bs2J8_30", "requests_per_step": REQ_PER_STEP,
+                 "mix": MIX, "atoms_log_uniform": [16, 32768]}
+    elif args.workload == "batch512":
+        from libdescriptor_b200 import batch as B
+
+        cfgs = B.diamond_batch(512, seed=1)
+        specs = {"sf24": sf24_spec(["Si"]), "bs6": bs_spec(6, ["Si"], [1.0])}
+
+        def one(budget):
+            secs, s = 0.0, []
+            for k, spec in specs.items():
+                r, n, _ = cpu_rate(spec, cfgs, budget_s=budget / 2)
+                secs += 1.0 / r
+                s.append(f"{n} centres ({k})")
+            return 1.0 / secs, ", ".join(s), threads
+
+        cdesc = {"workload": "batched_512_diamond_cells_sf24_and_bs2J6", "cells": 512}
+    else:
+        cfg, spec, cdesc = make_workload(args.workload, seed=1)
+
+        def one(budget):
+            return cpu_rate(spec, [cfg], budget_s=budget)
+
+    for _ in range(args.warmup):
+        one(1.0)
+    walls = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        r, sample, _ = one(6.0)
+        walls.append(time.perf_counter() - t0)
+        rates.append(r)
+    value = statistics.mean(rates)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "atoms/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(walls),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": cdesc,
+        "cpu_baseline": {"value": value, "unit": "atoms/s", "cores": threads, "kind": "port",
+                         "sample": f"per step about 6 s of desc+VJP work: {sample}, by the oracle's analytic "
+                                   f"adjoint (the reference's Enzyme gradient cannot be built offline)"},
+        "e2e": {"value": value, "unit": "atoms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------- GPU
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=None)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--workload", default="serve", choices=["serve", "batch512", "bs8", "sf24"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.steps is None:
+        args.steps = {"serve": 10, "batch512": 20}.get(args.workload, 200)
+        if args.impl == "reference":
+            args.steps = 3
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+
+    import libdescriptor_b200 as lds
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    runner = {"serve": run_serve, "batch512": run_batch512}.get(args.workload, run_single)
+    line = runner(args, torch, lds, dev, world, rank, local, dist)
+    if line is not None:
+        print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()

@@ -167,6 +167,73 @@ int ld_gradient_dev(ld_descriptor *d, int n_rows, const int *row_centre,
                     const double *dE_ddesc, double *d_coords, double *desc_out,
                     const int *image, ld_stream stream);
 
+/* Batched / served form of ld_compute_dev and ld_gradient_dev (no
+ * counterpart in the reference; its compute_batch / gradient_batch,
+ * src/Descriptors.cpp:138-163 and 190-215, loop over configurations on the
+ * host).  Row r's neighbours are neighbor_list[nbl_begin[r] ..
+ * nbl_begin[r] + (neigh_offsets[r+1] - neigh_offsets[r])): the rows of
+ * many configurations held anywhere in one resident neighbour arena are
+ * batched into one launch without copying their lists.  neigh_offsets is
+ * the exclusive prefix sum of the rows' neighbour counts in batch order;
+ * row_centre (required here) holds the rows' centre atoms in the same
+ * coordinate arena that the neighbour indices address. */
+int ld_compute_rows_dev(ld_descriptor *d, int n_rows, const int *row_centre,
+                        const long long *nbl_begin, const int *species,
+                        const int *neighbor_list, const long long *neigh_offsets,
+                        int max_neigh, const double *coords, double *desc,
+                        void *work, size_t work_bytes, ld_stream stream);
+int ld_gradient_rows_dev(ld_descriptor *d, int n_rows, const int *row_centre,
+                         const long long *nbl_begin, const int *species,
+                         const int *neighbor_list, const long long *neigh_offsets,
+                         int max_neigh, const double *coords,
+                         const double *dE_ddesc, double *d_coords, double *desc_out,
+                         const int *image, void *work, size_t work_bytes,
+                         ld_stream stream);
+
+/* Device work space (bytes, 256-byte aligned start required) that one
+ * ld_compute_rows_dev (vjp = 0) or ld_gradient_rows_dev (vjp = 1) call over
+ * n_rows rows needs when the caller passes `work`.  With work == NULL those
+ * calls take it by stream-ordered allocation; a caller-owned work space keeps
+ * the calls free of allocations (CUDA-graph capture, serving arenas).  One
+ * work space serves one call in flight at a time. */
+int ld_rows_work_bytes(const ld_descriptor *d, int n_rows, int vjp, size_t *bytes);
+
+/* Launch-shape tuning of one descriptor (no counterpart in the reference).
+ * Values <= 0 restore the built-in choice.  Results do not depend on the
+ * tuning except for the order of floating-point atomic additions. */
+#define LD_TUNE_SF_WARPS 0        /* symmetry functions: warps per CTA (1, 2, 4) */
+#define LD_TUNE_CTAS_PER_SM 1     /* per-centre kernels: resident CTA cap per SM */
+#define LD_TUNE_PAIR_GRID_MULT 2  /* bispectrum pair kernel: grid cap / (SMs x occupancy) */
+#define LD_TUNE_DYNAMIC_QUEUE 3   /* 1: centres claimed from an atomic counter   */
+int ld_set_tuning(ld_descriptor *d, int key, int value);
+int ld_get_tuning(const ld_descriptor *d, int key, int *value);
+
+/* Serving runtime (no counterpart in the reference): staging of one request
+ * into resident device rings.  The request's arrays are host arrays in the
+ * reference's layout with local indices (coords[n_total*3], species and
+ * image[n_total] with image = master row in 0..n_atoms-1,
+ * number_of_neighs[n_atoms], neighbor_list[nnz] into 0..n_total-1,
+ * dE_ddesc[n_atoms*width]).  ld_stage_request checks the indices, writes the
+ * fields into `staging` (pinned host memory, 256-byte aligned, at least
+ * ld_stage_bytes) with every index rebased to the ring slots row0 / atom0 /
+ * entry0, and enqueues the uploads on `stream`:
+ *   d_coords[atom0..], d_species[atom0..], d_image[atom0..] (= row0 + image),
+ *   d_nbl[entry0..] (= atom0 + neighbour), d_centre[row0..] (= atom0 + j),
+ *   d_begin[row0..] (= entry0 + exclusive prefix of the counts),
+ *   d_counts[row0..], d_dE[row0*width..].
+ * The staging memory may be reused once the stream has passed the uploads.
+ * The staged rows then join batches of ld_gradient_rows_dev over the rings
+ * (row_centre = d_centre, nbl_begin = d_begin, image = d_image). */
+int ld_stage_bytes(int n_atoms, int n_total, long long nnz, int width, size_t *bytes);
+int ld_stage_request(int n_atoms, int n_total, long long nnz, int width,
+                     int row0, int atom0, long long entry0,
+                     const double *coords, const int *species, const int *image,
+                     const int *neighbor_list, const int *number_of_neighs,
+                     const double *dE_ddesc, void *staging, size_t staging_bytes,
+                     double *d_coords, int *d_species, int *d_image, int *d_nbl,
+                     int *d_centre, long long *d_begin, int *d_counts, double *d_dE,
+                     ld_stream stream);
+
 /* Descriptor + VJP pass that allocates no device memory (no counterpart in
  * the reference; it serves callers that cannot call cudaMalloc while they
  * evaluate forces, e.g. engines whose device memory is owned by their own

@@ -141,8 +141,8 @@ __global__ void __launch_bounds__(NT) bs_kernel(BSDev p, RowArgs a, int cap) {
     for (int row = blockIdx.x; row < a.n_rows; row += gridDim.x) {
         const int i = a.row_centre ? a.row_centre[row] : row;
         const int lrow = a.row_list ? a.row_list[row] : row;
-        const long long off = a.off[lrow];
-        const int n = (int)(a.off[lrow + 1] - off);
+        const long long off = a.nbl_begin ? a.nbl_begin[lrow] : a.off[lrow];
+        const int n = (int)(a.off[lrow + 1] - a.off[lrow]);
         double *const dco = VJP ? a.dcoords + (size_t)row * a.dc_stride : nullptr;
         if (n > cap || n < 0 || (a.n_total > 0 && (i < 0 || i >= a.n_total))) {
             if (tid == 0) raise_status(a.status, n > cap ? kDevCapacity : kDevBadIndex);
@@ -608,6 +608,11 @@ static int bs2_dispatch(const BSDev &p, const RowArgs &a, cudaStream_t s) {
     case 10: return bs2_launch_t<10>(p, a, s);
     }
     return fail(LD_ERR_CAPACITY, "bispectrum: twojmax outside the compiled range");
+}
+
+size_t bs_work_bytes(const BSDev &p, int n_rows, bool vjp) {
+    const size_t y = vjp ? ((sizeof(double2) * (size_t)(n_rows > 0 ? n_rows : 0) * p.nL + 16 + 255) & ~(size_t)255) : 0;
+    return y + 256;
 }
 
 int bs_launch(const BSDev &p, const RowArgs &a, cudaStream_t s) {

@@ -8,6 +8,7 @@
 #include <cstring>
 #include <fstream>
 #include <map>
+#include <cstdint>
 #include <mutex>
 #include <queue>
 #include <set>
@@ -132,6 +133,8 @@ struct ld_descriptor {
     std::vector<int> bs_out_j1, bs_out_j2, bs_out_j;
     long long bs_inner_fwd = 0, bs_inner_vjp = 0;  // CG inner iterations per centre
     int bs_tasks_fwd = 0, bs_tasks_vjp = 0;
+    // launch-shape tuning (LD_TUNE_*), 0 = built-in choice
+    int tune[4] = {0, 0, 0, 0};
 };
 
 namespace ldb {
@@ -555,7 +558,13 @@ static int validate(const ld_descriptor *d, const HostRows &h, int n_total, cons
     return LD_OK;
 }
 
-int launch_rows(ld_descriptor *d, const RowArgs &a, cudaStream_t s) {
+int launch_rows(ld_descriptor *d, const RowArgs &a0, cudaStream_t s) {
+    RowArgs a = a0;
+    a.sf_warps = d->tune[LD_TUNE_SF_WARPS];
+    a.ctas_per_sm = d->tune[LD_TUNE_CTAS_PER_SM];
+    a.pair_grid_mult = d->tune[LD_TUNE_PAIR_GRID_MULT];
+    // the allocation-free entry point never takes the queue counter
+    a.dynamic_queue = a0.fused_only ? 0 : d->tune[LD_TUNE_DYNAMIC_QUEUE];
     if (d->kind == LD_KIND_SYMMETRY_FUNCTIONS) return sf_launch(d->sf, a, s);
     return bs_launch(d->bs, a, s);
 }
@@ -1059,7 +1068,8 @@ int ld_neighbor_offsets_dev(ld_descriptor *d, int n_rows, const int *number_of_n
 
 static int dev_pass(ld_descriptor *d, int n_rows, const int *row_centre, const int *species, const int *nbl,
                     const long long *off, int max_neigh, const double *coords, double *desc, const double *dE,
-                    double *dcoords, const int *image, ld_stream stream) {
+                    double *dcoords, const int *image, ld_stream stream, const long long *nbl_begin = nullptr,
+                    void *work = nullptr, size_t work_bytes = 0) {
     if (!d) return fail(LD_ERR_INVALID_ARG, "descriptor handle is NULL");
     if (n_rows < 0 || max_neigh < 0) return fail(LD_ERR_INVALID_ARG, "negative size");
     if (n_rows == 0) return LD_OK;
@@ -1081,7 +1091,67 @@ static int dev_pass(ld_descriptor *d, int n_rows, const int *row_centre, const i
     a.dcoords = dcoords;
     a.image = image;
     a.status = d->status.as<int>();
+    a.nbl_begin = nbl_begin;
+    if (work) {
+        if (reinterpret_cast<std::uintptr_t>(work) & 255)
+            return fail(LD_ERR_INVALID_ARG, "work space must start on a 256-byte boundary");
+        size_t need = 0;
+        int rc2 = ld_rows_work_bytes(d, n_rows, dE ? 1 : 0, &need);
+        if (rc2) return rc2;
+        if (work_bytes < need)
+            return fail(LD_ERR_INVALID_ARG, "work space of " + std::to_string(work_bytes) + " bytes < " +
+                                                std::to_string(need) + " needed");
+        a.work = work;
+        a.work_bytes = work_bytes;
+    }
     return launch_rows(d, a, (cudaStream_t)stream);
+}
+
+int ld_rows_work_bytes(const ld_descriptor *d, int n_rows, int vjp, size_t *bytes) {
+    if (!d || !bytes || n_rows < 0) return fail(LD_ERR_INVALID_ARG, "ld_rows_work_bytes: bad arguments");
+    *bytes = d->kind == LD_KIND_SYMMETRY_FUNCTIONS ? sf_work_bytes(d->sf, n_rows, vjp != 0)
+                                                   : bs_work_bytes(d->bs, n_rows, vjp != 0);
+    return LD_OK;
+}
+
+int ld_compute_rows_dev(ld_descriptor *d, int n_rows, const int *row_centre, const long long *nbl_begin,
+                        const int *species, const int *neighbor_list, const long long *neigh_offsets,
+                        int max_neigh, const double *coords, double *desc, void *work, size_t work_bytes,
+                        ld_stream stream) {
+    if (n_rows > 0 && (!row_centre || !nbl_begin))
+        return fail(LD_ERR_INVALID_ARG, "ld_compute_rows_dev: row_centre and nbl_begin are required");
+    return dev_pass(d, n_rows, row_centre, species, neighbor_list, neigh_offsets, max_neigh, coords, desc, nullptr,
+                    nullptr, nullptr, stream, nbl_begin, work, work_bytes);
+}
+
+int ld_gradient_rows_dev(ld_descriptor *d, int n_rows, const int *row_centre, const long long *nbl_begin,
+                         const int *species, const int *neighbor_list, const long long *neigh_offsets,
+                         int max_neigh, const double *coords, const double *dE_ddesc, double *d_coords,
+                         double *desc_out, const int *image, void *work, size_t work_bytes, ld_stream stream) {
+    if (n_rows > 0 && (!row_centre || !nbl_begin))
+        return fail(LD_ERR_INVALID_ARG, "ld_gradient_rows_dev: row_centre and nbl_begin are required");
+    if (n_rows > 0 && !dE_ddesc) return fail(LD_ERR_INVALID_ARG, "dE_ddesc is NULL");
+    return dev_pass(d, n_rows, row_centre, species, neighbor_list, neigh_offsets, max_neigh, coords, desc_out,
+                    dE_ddesc, d_coords, image, stream, nbl_begin, work, work_bytes);
+}
+
+int ld_set_tuning(ld_descriptor *d, int key, int value) {
+    if (!d) return fail(LD_ERR_INVALID_ARG, "descriptor handle is NULL");
+    if (key < 0 || key > LD_TUNE_DYNAMIC_QUEUE) return fail(LD_ERR_INVALID_ARG, "unknown tuning key");
+    if (value < 0) value = 0;
+    if (key == LD_TUNE_SF_WARPS && value != 0 && value != 1 && value != 2 && value != 4)
+        return fail(LD_ERR_INVALID_ARG, "LD_TUNE_SF_WARPS must be 1, 2 or 4");
+    if (key == LD_TUNE_DYNAMIC_QUEUE) value = value ? 1 : 0;
+    std::lock_guard<std::mutex> lk(d->mu);
+    d->tune[key] = value;
+    return LD_OK;
+}
+
+int ld_get_tuning(const ld_descriptor *d, int key, int *value) {
+    if (!d || !value) return fail(LD_ERR_INVALID_ARG, "NULL argument");
+    if (key < 0 || key > LD_TUNE_DYNAMIC_QUEUE) return fail(LD_ERR_INVALID_ARG, "unknown tuning key");
+    *value = d->tune[key];
+    return LD_OK;
 }
 
 int ld_compute_dev(ld_descriptor *d, int n_rows, const int *row_centre, const int *species, const int *neighbor_list,

@@ -124,6 +124,17 @@ struct RowArgs {
     const int *image = nullptr;
     int *status = nullptr;             // device error word
     bool fused_only = false;           // gradient in one kernel, no work space (no allocation)
+    // ragged batches: start of each row's neighbours in nbl (nullable: off[row]);
+    // off[] then only numbers the rows' neighbours consecutively
+    const long long *nbl_begin = nullptr;
+    // launch shape (0 = automatic); set through ld_set_tuning
+    int sf_warps = 0;                  // warps (centre rows) per symmetry-function CTA: 1, 2, 4
+    int ctas_per_sm = 0;               // per-centre bispectrum CTAs per SM
+    int pair_grid_mult = 0;            // pair-parallel gradient grid = SMs x occupancy x this
+    int dynamic_queue = 0;
+    // caller-provided device work space (nullable: stream-ordered allocation)
+    void *work = nullptr;
+    size_t work_bytes = 0;             // 1: rows claimed from an atomic counter instead of grid stride
 };
 
 // warps of the twojmax-specialised per-centre bispectrum CTA (4..8)
@@ -135,6 +146,8 @@ constexpr int bs2_warps(int J) {
 
 int sf_launch(const SFDev &p, const RowArgs &a, cudaStream_t s);
 int bs_launch(const BSDev &p, const RowArgs &a, cudaStream_t s);
+size_t sf_work_bytes(const SFDev &p, int n_rows, bool vjp);
+size_t bs_work_bytes(const BSDev &p, int n_rows, bool vjp);
 size_t bs_smem_bytes(const BSDev &p, int max_neigh, bool vjp);
 
 int offsets_launch(int n_rows, const int *counts, long long *off, int *maxn,

@@ -364,6 +364,61 @@ PYBIND11_MODULE(_libdescriptor, m) {
                               (const long long *)off, max_neigh, (const double *)coords, (const double *)dE,
                               (double *)dcoords, (double *)desc, (const int *)image, (ld_stream)stream));
     });
+    m.def("_compute_rows_dev", [](Kind &ds, int n_rows, std::uintptr_t row_centre, std::uintptr_t nbl_begin,
+                                  std::uintptr_t species, std::uintptr_t nbl, std::uintptr_t off, int max_neigh,
+                                  std::uintptr_t coords, std::uintptr_t desc, std::uintptr_t work,
+                                  std::size_t work_bytes, std::uintptr_t stream) {
+        check(ld_compute_rows_dev(ds.get(), n_rows, (const int *)row_centre, (const long long *)nbl_begin,
+                                  (const int *)species, (const int *)nbl, (const long long *)off, max_neigh,
+                                  (const double *)coords, (double *)desc, (void *)work, work_bytes,
+                                  (ld_stream)stream));
+    });
+    m.def("_gradient_rows_dev", [](Kind &ds, int n_rows, std::uintptr_t row_centre, std::uintptr_t nbl_begin,
+                                   std::uintptr_t species, std::uintptr_t nbl, std::uintptr_t off, int max_neigh,
+                                   std::uintptr_t coords, std::uintptr_t dE, std::uintptr_t dcoords,
+                                   std::uintptr_t desc, std::uintptr_t image, std::uintptr_t work,
+                                   std::size_t work_bytes, std::uintptr_t stream) {
+        check(ld_gradient_rows_dev(ds.get(), n_rows, (const int *)row_centre, (const long long *)nbl_begin,
+                                   (const int *)species, (const int *)nbl, (const long long *)off, max_neigh,
+                                   (const double *)coords, (const double *)dE, (double *)dcoords, (double *)desc,
+                                   (const int *)image, (void *)work, work_bytes, (ld_stream)stream));
+    });
+    m.def("_rows_work_bytes", [](Kind &ds, int n_rows, bool vjp) {
+        std::size_t b = 0;
+        check(ld_rows_work_bytes(ds.get(), n_rows, vjp ? 1 : 0, &b));
+        return b;
+    });
+    m.def("_stage_bytes", [](int n, int nt, long long nnz, int width) {
+        std::size_t b = 0;
+        check(ld_stage_bytes(n, nt, nnz, width, &b));
+        return b;
+    });
+    m.def("_stage_request", [](int n, int nt, long long nnz, int width, int row0, int atom0, long long entry0,
+                               DArr coords, IArr species, IArr image, IArr nbl, IArr counts, DArr dE,
+                               std::uintptr_t staging, std::size_t staging_bytes, std::uintptr_t d_coords,
+                               std::uintptr_t d_species, std::uintptr_t d_image, std::uintptr_t d_nbl,
+                               std::uintptr_t d_centre, std::uintptr_t d_begin, std::uintptr_t d_counts,
+                               std::uintptr_t d_dE, std::uintptr_t stream) {
+        if ((long long)coords.size() < 3LL * nt || (long long)species.size() < nt || (long long)image.size() < nt ||
+            (long long)nbl.size() < nnz || (long long)counts.size() < n || (long long)dE.size() < (long long)n * width)
+            throw py::value_error("_stage_request: arrays shorter than the stated sizes");
+        int rc;
+        {
+            py::gil_scoped_release nogil;
+            rc = ld_stage_request(n, nt, nnz, width, row0, atom0, entry0, coords.data(), species.data(),
+                                  image.data(), nnz ? nbl.data() : nullptr, counts.data(), dE.data(),
+                                  (void *)staging, staging_bytes, (double *)d_coords, (int *)d_species,
+                                  (int *)d_image, (int *)d_nbl, (int *)d_centre, (long long *)d_begin,
+                                  (int *)d_counts, (double *)d_dE, (ld_stream)stream);
+        }
+        check(rc);
+    });
+    m.def("_set_tuning", [](Kind &ds, int key, int value) { check(ld_set_tuning(ds.get(), key, value)); });
+    m.def("_get_tuning", [](Kind &ds, int key) {
+        int v = 0;
+        check(ld_get_tuning(ds.get(), key, &v));
+        return v;
+    });
     m.def("_neighbor_offsets_dev", [](Kind &ds, int n_rows, std::uintptr_t counts, std::uintptr_t off,
                                       bool want_max, std::uintptr_t stream) {
         int mx = 0;

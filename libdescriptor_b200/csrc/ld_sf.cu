@@ -77,7 +77,7 @@ __device__ __forceinline__ WarpSlice slice(double *base, int cap, bool vjp) {
 
 template <bool VJP, int M2, int M3>
 __global__ void __launch_bounds__(kSFThreads, VJP ? 3 : 4)
-sf_kernel(SFDev p, RowArgs a, int per_warp_doubles) {
+sf_kernel(SFDev p, RowArgs a, int per_warp_doubles, int *queue) {
     extern __shared__ double smem[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -86,16 +86,31 @@ sf_kernel(SFDev p, RowArgs a, int per_warp_doubles) {
     WarpSlice S = slice(smem + (size_t)warp * per_warp_doubles, cap, VJP);
     const int width = p.width;
 
-    for (int row = blockIdx.x * nw + warp; row < a.n_rows; row += gridDim.x * nw) {
+    int row = blockIdx.x * nw + warp;
+    if (queue) {
+        int r0 = 0;
+        if (lane == 0) r0 = atomicAdd(queue, 1);
+        row = __shfl_sync(0xffffffffu, r0, 0);
+    }
+    for (; row < a.n_rows;) {
         const int i = a.row_centre ? a.row_centre[row] : row;
         const int lrow = a.row_list ? a.row_list[row] : row;
-        const long long off = a.off[lrow];
-        const int n = (int)(a.off[lrow + 1] - off);
-        double *const dco = VJP ? a.dcoords + (size_t)row * a.dc_stride : nullptr;
+        const long long off = a.nbl_begin ? a.nbl_begin[lrow] : a.off[lrow];
+        const int n = (int)(a.off[lrow + 1] - a.off[lrow]);
+        const int cur_row = row;  // row being processed; `row` is the next one
+        // next row: from the shared counter (dynamic) or by grid stride
+        if (queue) {
+            int r1 = 0;
+            if (lane == 0) r1 = atomicAdd(queue, 1);
+            row = __shfl_sync(0xffffffffu, r1, 0);
+        } else {
+            row += gridDim.x * nw;
+        }
+        double *const dco = VJP ? a.dcoords + (size_t)cur_row * a.dc_stride : nullptr;
         if (n > cap || n < 0 || (a.n_total > 0 && (i < 0 || i >= a.n_total))) {
             raise_status(a.status, n > cap ? kDevCapacity : kDevBadIndex);
             if (a.desc)
-                for (int q = lane; q < width; q += 32) a.desc[(size_t)row * width + q] = __longlong_as_double(0x7ff8000000000000LL);
+                for (int q = lane; q < width; q += 32) a.desc[(size_t)cur_row * width + q] = __longlong_as_double(0x7ff8000000000000LL);
             continue;
         }
         const double cix = a.coords[3 * i], ciy = a.coords[3 * i + 1], ciz = a.coords[3 * i + 2];
@@ -133,7 +148,7 @@ sf_kernel(SFDev p, RowArgs a, int per_warp_doubles) {
             }
         }
         __syncwarp();
-        const double *dE = VJP ? a.dE + (size_t)row * width : nullptr;
+        const double *dE = VJP ? a.dE + (size_t)cur_row * width : nullptr;
         double gix = 0.0, giy = 0.0, giz = 0.0;
         // ---- two-body terms (g1, g2, g3)
         if (p.n2 > 0) {
@@ -184,7 +199,7 @@ sf_kernel(SFDev p, RowArgs a, int per_warp_doubles) {
             for (int q = 0; q < M2; ++q) {
                 if (q < p.n2) {
                     const double v = warp_sum(acc2[q]);
-                    if (lane == 0 && a.desc) a.desc[(size_t)row * width + __ldg(p.o2 + q)] = v;
+                    if (lane == 0 && a.desc) a.desc[(size_t)cur_row * width + __ldg(p.o2 + q)] = v;
                 }
             }
         }
@@ -343,7 +358,7 @@ sf_kernel(SFDev p, RowArgs a, int per_warp_doubles) {
             for (int q = 0; q < M3; ++q) {
                 if (q < p.n3) {
                     const double v = warp_sum(acc3[q]);
-                    if (lane == 0 && a.desc) a.desc[(size_t)row * width + __ldg(p.o3 + q)] = v;
+                    if (lane == 0 && a.desc) a.desc[(size_t)cur_row * width + __ldg(p.o3 + q)] = v;
                 }
             }
         }
@@ -377,7 +392,7 @@ int launch_t(const SFDev &p, const RowArgs &a, cudaStream_t s) {
     const int ndbl = cap * (VJP ? 11 : 7);
     const int per_warp = ndbl + (3 * cap + 1) / 2 + 2;  // doubles (ints packed after)
     const size_t per_warp_bytes = (size_t)per_warp * sizeof(double);
-    int nw = 4;
+    int nw = (a.sf_warps == 1 || a.sf_warps == 2 || a.sf_warps == 4) ? a.sf_warps : 4;
     while (nw > 1 && per_warp_bytes * nw > 200 * 1024) --nw;
     if (per_warp_bytes * nw > 220 * 1024)
         return fail(LD_ERR_CAPACITY, "symmetry functions: max_neigh=" + std::to_string(a.max_neigh) +
@@ -390,18 +405,38 @@ int launch_t(const SFDev &p, const RowArgs &a, cudaStream_t s) {
     LDB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     LDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, nw * 32, smem));
     if (per_sm < 1) per_sm = 1;
+    if (a.ctas_per_sm > 0 && a.ctas_per_sm < per_sm) per_sm = a.ctas_per_sm;
     const int rows_per_block = nw;
     long long want = (a.n_rows + rows_per_block - 1) / rows_per_block;
     long long grid = (long long)nsm * per_sm;
     if (want < grid) grid = want;
     if (grid < 1) grid = 1;
-    kern<<<(unsigned)grid, nw * 32, smem, s>>>(p, a, per_warp);
+    int *queue = nullptr;
+    bool own = false;
+    if (a.dynamic_queue) {
+        if (a.work) {
+            if (a.work_bytes < sizeof(int)) return fail(LD_ERR_INVALID_ARG, "work space too small");
+            queue = static_cast<int *>(a.work);
+        } else {
+            LDB_CUDA(cudaMallocAsync((void **)&queue, sizeof(int), s));
+            own = true;
+        }
+        LDB_CUDA(cudaMemsetAsync(queue, 0, sizeof(int), s));
+    }
+    kern<<<(unsigned)grid, nw * 32, smem, s>>>(p, a, per_warp, queue);
     count_launch();
-    LDB_CUDA(cudaGetLastError());
+    cudaError_t e = cudaGetLastError();
+    if (own) {
+        cudaError_t e2 = cudaFreeAsync(queue, s);
+        if (e == cudaSuccess) e = e2;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "sf_kernel");
     return LD_OK;
 }
 
 }  // namespace
+
+size_t sf_work_bytes(const SFDev &, int, bool) { return 256; }
 
 int sf_launch(const SFDev &p, const RowArgs &a, cudaStream_t s) {
     if (a.n_rows <= 0) return LD_OK;

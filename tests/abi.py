@@ -81,6 +81,16 @@ class Abi:
             L.ld_sync_status.argtypes = [C.c_void_p, C.c_void_p]
             L.ld_neighbor_offsets_dev.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
                                                   C.POINTER(C.c_int), C.c_void_p]
+            L.ld_compute_rows_dev.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                              C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                              C.c_void_p, C.c_size_t, C.c_void_p]
+            L.ld_gradient_rows_dev.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                               C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                               C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t,
+                                               C.c_void_p]
+            L.ld_rows_work_bytes.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_size_t)]
+            L.ld_set_tuning.argtypes = [C.c_void_p, C.c_int, C.c_int]
+            L.ld_get_tuning.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
             cls._lib = L
         return cls._lib
 
@@ -183,3 +193,16 @@ class Handle:
         Abi.check(Abi.lib().ld_jacobian(self.h, int(n_atoms), coords.shape[0], _i(species), _i(nbl),
                                         _i(counts), coords.ravel(), J))
         return J
+
+    def set_tuning(self, key, value):
+        Abi.check(Abi.lib().ld_set_tuning(self.h, int(key), int(value)))
+
+    def get_tuning(self, key):
+        v = C.c_int()
+        Abi.check(Abi.lib().ld_get_tuning(self.h, int(key), C.byref(v)))
+        return v.value
+
+    def rows_work_bytes(self, n_rows, vjp):
+        b = C.c_size_t()
+        Abi.check(Abi.lib().ld_rows_work_bytes(self.h, int(n_rows), int(vjp), C.byref(b)))
+        return b.value

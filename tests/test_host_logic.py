@@ -1,0 +1,230 @@
+"""CPU: host-side logic of the serving loop (rings, admission by footprint,
+continuous batching, retirement order) driven by a fake device, and the
+autotuner's candidate space and cache."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from libdescriptor_b200 import serving as S
+
+
+# ----------------------------------------------------------------- rings
+def _occupied(ring):
+    occ = np.zeros(ring.cap, dtype=int)
+    for s, n in ring.live:
+        occ[s:s + n] += 1
+    return occ
+
+
+def test_ring_random_ops_never_overlap():
+    rng = np.random.default_rng(0)
+    for cap in (1, 7, 64, 1000):
+        ring = S.Ring(cap)
+        for _ in range(3000):
+            if ring.live and rng.random() < 0.45:
+                ring.free(ring.live[0][0])
+            else:
+                n = int(rng.integers(1, max(2, cap // 3 + 1)))
+                s = ring.alloc(n)
+                if s is not None:
+                    assert 0 <= s and s + n <= cap
+            occ = _occupied(ring)
+            assert occ.max(initial=0) <= 1, "overlapping ranges"
+
+
+def test_ring_fifo_and_wrap():
+    r = S.Ring(10)
+    a = r.alloc(4)
+    b = r.alloc(4)
+    assert (a, b) == (0, 4)
+    assert r.alloc(3) is None          # only 2 left at the end, 0 at the start
+    r.free(a)
+    c = r.alloc(3)                     # wraps to the start
+    assert c == 0
+    assert r.alloc(2) is None          # [3, 4) free but only 1 slot; the end [8, 10) is behind the wrap
+    with pytest.raises(RuntimeError):
+        r.free(c)                      # not the oldest
+    r.free(b)
+    r.free(c)
+    assert r.alloc(10) == 0
+
+
+def test_ring_rejects_oversize():
+    r = S.Ring(5)
+    assert r.alloc(6) is None
+    assert not r.fits_ever(6)
+
+
+# ------------------------------------------------------------ scheduler
+class FakeDevice:
+    """Backend that records calls; a batch finishes when release() says so."""
+
+    def __init__(self):
+        self.staged = []
+        self.launched = []
+        self.finished = set()
+
+    def stage(self, req):
+        self.staged.append(req.rid)
+
+    def launch(self, plan):
+        plan.handle = len(self.launched)
+        self.launched.append(plan)
+
+    def done(self, plan):
+        return plan.handle in self.finished
+
+    def finish(self, plan):
+        for r in plan.reqs:
+            r.desc = ("desc", r.rid)
+
+    def release_all(self):
+        self.finished.update(p.handle for p in self.launched)
+
+
+def _req(rid, lane, n, nt=None, nnz=None):
+    nt = nt or n
+    nnz = n * 4 if nnz is None else nnz
+    return S.Request(rid, lane, n, np.zeros((nt, 3)), np.zeros(nt, np.int32), np.arange(nt, dtype=np.int32) % n,
+                     np.full(n, nnz // n, np.int32), np.zeros(nnz, np.int32), np.zeros((n, 2)))
+
+
+def test_admission_waits_for_memory_and_batches_continuously():
+    caps = {"sf": S.LaneCaps(rows=100, atoms=300, entries=400), "bs": S.LaneCaps(rows=50, atoms=150, entries=200)}
+    dev = FakeDevice()
+    sch = S.Scheduler(caps, dev, max_batch_rows=64, depth=2, out_rows=128)
+    reqs = [_req(i, "sf" if i % 3 else "bs", 20) for i in range(12)]
+    for r in reqs:
+        sch.submit(r)
+    sch.admit(0.0)
+    # sf: 8 requests x 20 rows, ring of 100 -> 5 admitted; bs: 4 x 20, ring of 50 -> 2
+    assert len(sch.admitted["sf"]) == 5 and len(sch.pending["sf"]) == 3
+    assert len(sch.admitted["bs"]) == 2 and len(sch.pending["bs"]) == 2
+    sch.launch()
+    # max 64 rows per batch: sf batches of 3 and 2 requests, bs one batch of 2
+    sizes = sorted((p.lane, len(p.reqs)) for p in dev.launched)
+    assert sizes == [("bs", 2), ("sf", 2), ("sf", 3)]
+    for p in dev.launched:
+        assert p.n_rows == sum(r.n_atoms for r in p.reqs)
+        assert [r.slots[0] for r in p.reqs] == [p.row0 + 20 * i for i in range(len(p.reqs))]
+    # nothing completes until the device says so; then memory frees and the
+    # waiting requests are admitted and launched
+    assert sch.poll(1.0) == []
+    dev.release_all()
+    done = sch.poll(2.0)
+    assert sorted(r.rid for r in done) == sorted(r.rid for p in dev.launched for r in p.reqs)
+    assert all(r.done_at == 2.0 for r in done)
+    sch.admit(2.0)
+    sch.launch()
+    while not sch.idle():
+        dev.release_all()
+        sch.step(3.0)
+    assert sorted(r.rid for r in sch.completed) == list(range(12))
+    # FIFO per lane
+    for lane in ("sf", "bs"):
+        rids = [r.rid for r in sch.completed if r.lane == lane]
+        assert rids == sorted(rids)
+    assert all(ring.used == 0 for rings in sch.rings.values() for ring in rings)
+
+
+def test_oversized_request_is_rejected_up_front():
+    caps = {"sf": S.LaneCaps(rows=10, atoms=30, entries=40)}
+    sch = S.Scheduler(caps, FakeDevice(), max_batch_rows=8, out_rows=16)
+    with pytest.raises(ValueError):
+        sch.submit(_req(0, "sf", 11))
+    with pytest.raises(ValueError):
+        sch.submit(_req(1, "sf", 9))       # more rows than one batch
+
+
+def test_batch_stops_at_row_ring_wrap():
+    caps = {"sf": S.LaneCaps(rows=50, atoms=1000, entries=1000)}
+    dev = FakeDevice()
+    sch = S.Scheduler(caps, dev, max_batch_rows=50, depth=1, out_rows=100)
+    for i in range(2):
+        sch.submit(_req(i, "sf", 20))
+    sch.step(0.0)                       # admits 0, 1; launches [0, 1]
+    dev.release_all()
+    sch.submit(_req(2, "sf", 20))       # rows 40..50 too short -> wraps to 0
+    sch.submit(_req(3, "sf", 5))
+    sch.step(1.0)
+    assert [r.slots[0] for r in (sch.completed[0], sch.completed[1])] == [0, 20]
+    last = dev.launched[-1]
+    assert [r.rid for r in last.reqs] == [2, 3] and last.row0 == 0
+
+
+def test_plan_caps_respects_budget():
+    caps = S.plan_caps(1 << 30, {"sf": 24, "bs": 55}, {"sf": 1.0, "bs": 1.0}, {"sf": 1 << 20, "bs": 1 << 25})
+    used = 0
+    for k, w in (("sf", 24), ("bs", 55)):
+        c = caps[k]
+        used += c.rows * S.lane_bytes_per_row(w) + c.atoms * 32 + c.entries * 4
+    assert used + (1 << 20) + (1 << 25) <= 1 << 30
+    with pytest.raises(ValueError):
+        S.plan_caps(1 << 20, {"sf": 24}, {"sf": 1.0}, {"sf": 1 << 21})
+
+
+def test_fold_host_matches_add_at():
+    rng = np.random.default_rng(1)
+    n, nt = 13, 50
+    g = rng.normal(size=(nt, 3))
+    img = np.concatenate([np.arange(n), rng.integers(0, n, nt - n)]).astype(np.int32)
+    ref = g[:n].copy()
+    np.add.at(ref, img[n:], g[n:])
+    np.testing.assert_allclose(S.fold_host(g, n, img), ref, rtol=1e-14, atol=1e-14)
+
+
+def test_poisson_arrivals_rate():
+    a = S.poisson_arrivals(20000, 5000.0, seed=3)
+    assert np.all(np.diff(a) >= 0)
+    assert abs(len(a) / a[-1] - 5000.0) / 5000.0 < 0.03
+
+
+# ---------------------------------------------------------------- tuner
+def test_tuner_candidates_and_cache(tmp_path, monkeypatch):
+    from libdescriptor_b200 import tuner
+
+    sf = tuner.candidates(0)
+    bs = tuner.candidates(1)
+    assert {c["sf_warps"] for c in sf} == {1, 2, 4}
+    assert {c["dynamic_queue"] for c in sf + bs} == {0, 1}
+    assert {c["pair_grid_mult"] for c in bs} == {2, 4, 8, 16}
+    assert tuner.shape_key("B200", "x", 1000, 30) == tuner.shape_key("B200", "x", 1024, 30)
+    assert tuner.shape_key("B200", "x", 1025, 30) != tuner.shape_key("B200", "x", 1024, 30)
+
+    applied = []
+    monkeypatch.setattr(tuner.B, "set_tuning", lambda kind, shape: applied.append(dict(shape or {})))
+
+    class FakeTorchCuda:
+        @staticmethod
+        def get_device_name(dev):
+            return "FakeGPU"
+
+    class FakeTorch:
+        cuda = FakeTorchCuda
+
+    class FakeDB:
+        n_rows, max_neigh = 5000, 31
+
+    class FakeDesc:
+        device = None
+
+    class FakePass:
+        torch = FakeTorch
+        kind = object()
+        db = FakeDB
+        desc = FakeDesc
+
+    cost = {json.dumps(c, sort_keys=True): 1.0 + i for i, c in enumerate(bs)}
+    best_shape = bs[5]
+    cost[json.dumps(best_shape, sort_keys=True)] = 0.1
+    path = os.path.join(tmp_path, "tune.json")
+    t = tuner.Autotuner(cache_path=path)
+    monkeypatch.setattr(t, "time_shape", lambda p, shape: cost[json.dumps(shape, sort_keys=True)])
+    got = t.tune(FakePass, "bs8", 1)
+    assert got == best_shape and applied[-1] == best_shape
+    # cached: a fresh tuner reads the file and times nothing
+    t2 = tuner.Autotuner(cache_path=path)
+    monkeypatch.setattr(t2, "time_shape", lambda p, s: pytest.fail("timed a cached shape"))
+    assert t2.tune(FakePass, "bs8", 1) == best_shape
