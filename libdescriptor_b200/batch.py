@@ -24,7 +24,7 @@ import numpy as np
 from . import _ext
 from . import workloads as W
 
-TUNE_KEYS = {"sf_warps": 0, "ctas_per_sm": 1, "pair_grid_mult": 2, "dynamic_queue": 3}
+TUNE_KEYS = {"sf_warps": 0, "ctas_per_sm": 1, "pair_grid_mult": 2, "dynamic_queue": 3, "sf_generic": 4}
 
 
 def set_tuning(kind, tuning: dict | None) -> None:

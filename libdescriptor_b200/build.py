@@ -31,11 +31,13 @@ INCLUDE = os.path.join(ROOT, "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
-                     "-I" + INCLUDE, "-I" + CSRC]
+                     "-I" + INCLUDE, "-I" + CSRC] + os.environ.get("LDB_NVCC_DEFINES", "").split()
 CORE_SOURCES = ["ld_sf.cu", "ld_bs.cu", "ld_util.cu", "ld_core.cpp", "ld_neighbor.cpp", "ld_noalloc.cu",
                 "ld_bs2_j0_1_2_3_4.cu", "ld_bs2_j5_6.cu", "ld_bs2_j7.cu", "ld_bs2_j8.cu", "ld_bs2_j9.cu",
-                "ld_bs2_j10.cu", "ld_serve.cpp"]
-HEADERS = [os.path.join(CSRC, "ld_internal.h"), os.path.join(CSRC, "ld_bs2.cuh"),
+                "ld_bs2_j10.cu", "ld_serve.cpp", "ld_sfg.cu"]
+# host threads for the serving runtime's request staging
+EXTRA_FLAGS = {"ld_serve.cpp": ["-Xcompiler", "-fopenmp"]}
+HEADERS = [os.path.join(CSRC, "ld_internal.h"), os.path.join(CSRC, "ld_sf_common.cuh"), os.path.join(CSRC, "ld_bs2.cuh"),
            os.path.join(CSRC, "ld_bs2_impl.cuh"), os.path.join(INCLUDE, "libdescriptor_b200.h")]
 
 
@@ -72,13 +74,13 @@ def build(verbose: bool = False, jobs: int | None = None) -> None:
         o = os.path.join(OBJ, src + ".o")
         objs.append(o)
         if _stale(o, [s] + HEADERS):
-            todo.append([nvcc] + NVCC_FLAGS + ["-c", s, "-o", o])
+            todo.append([nvcc] + NVCC_FLAGS + EXTRA_FLAGS.get(src, []) + ["-c", s, "-o", o])
     if todo:
         with cf.ThreadPoolExecutor(max_workers=jobs or min(len(todo), os.cpu_count() or 4)) as ex:
             for f in [ex.submit(_run, c, verbose) for c in todo]:
                 f.result()
     if _stale(LIB, objs):
-        _run([nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lpthread"], verbose)
+        _run([nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lpthread", "-lgomp"], verbose)
     pyb = os.path.join(CSRC, "ld_pybind.cpp")
     if _stale(MOD, [pyb, LIB] + HEADERS):
         import pybind11

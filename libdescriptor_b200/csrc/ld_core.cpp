@@ -134,7 +134,7 @@ struct ld_descriptor {
     long long bs_inner_fwd = 0, bs_inner_vjp = 0;  // CG inner iterations per centre
     int bs_tasks_fwd = 0, bs_tasks_vjp = 0;
     // launch-shape tuning (LD_TUNE_*), 0 = built-in choice
-    int tune[4] = {0, 0, 0, 0};
+    int tune[5] = {0, 0, 0, 0, 0};
 };
 
 namespace ldb {
@@ -230,6 +230,67 @@ static int build_sf(ld_descriptor *d, int ns, const double *cutoff, int n_types,
     if ((int)o2.size() > 64 || (int)o3.size() > 64)
         return fail(LD_ERR_CAPACITY, "symmetry functions: at most 64 outputs of one body order are supported");
     SFDev &s = d->sf;
+    // factored (grid) form for the specialised kernel, when the set has one
+    {
+        SFGrid g;
+        bool ok = (int)o2.size() <= kSFG2;
+        g.n2 = (int)o2.size();
+        for (int q = 0; ok && q < g.n2; ++q) {
+            g.t2[q] = t2[q];
+            g.o2[q] = o2[q];
+            g.a2[q] = a2[q];
+            g.b2[q] = b2[q];
+        }
+        for (int ty = 0; ok && ty < 2; ++ty) {
+            const int tcode = ty == 0 ? 4 : 5;
+            std::vector<std::pair<double, double>> ang;   // (lambda, zeta), first appearance
+            std::vector<double> rad;                      // ascending eta
+            for (auto &q : three)
+                if (q.t == tcode) {
+                    if (std::find(ang.begin(), ang.end(), std::make_pair(q.lam, q.zeta)) == ang.end())
+                        ang.push_back({q.lam, q.zeta});
+                    if (std::find(rad.begin(), rad.end(), q.eta) == rad.end()) rad.push_back(q.eta);
+                }
+            std::sort(rad.begin(), rad.end());
+            if ((int)ang.size() > kSFGA || (int)rad.size() > kSFGR) {
+                ok = false;
+                break;
+            }
+            g.na[ty] = (int)ang.size();
+            g.nr[ty] = (int)rad.size();
+            for (int a = 0; a < kSFGA; ++a)
+                for (int r = 0; r < kSFGR; ++r) g.out[ty][a][r] = -1;
+            for (int a = 0; a < g.na[ty]; ++a) {
+                g.lam[ty][a] = ang[a].first;
+                g.zeta[ty][a] = ang[a].second;
+                g.P[ty][a] = std::pow(2, 1 - ang[a].second);
+                const double z = ang[a].second;
+                g.zi[ty][a] = (z >= 0 && z <= 64 && std::floor(z) == z) ? (int)z : -1;
+            }
+            for (int r = 0; r < g.nr[ty]; ++r) {
+                g.eta[ty][r] = rad[r];
+                int code = 0;
+                if (r > 0 && rad[0] > 0 && rad[r] > 0) {
+                    const double ratio = rad[r] / rad[0];
+                    const double k = std::floor(ratio + 0.5);
+                    if (k >= 2 && k <= 256 && std::fabs(ratio - k) <= 1e-9 * ratio) code = (int)k;
+                }
+                g.ec[ty][r] = code;
+            }
+            for (auto &q : three)
+                if (q.t == tcode) {
+                    const int a = (int)(std::find(ang.begin(), ang.end(), std::make_pair(q.lam, q.zeta)) - ang.begin());
+                    const int r = (int)(std::find(rad.begin(), rad.end(), q.eta) - rad.begin());
+                    if (g.out[ty][a][r] >= 0) {   // two outputs with identical parameters
+                        ok = false;
+                        break;
+                    }
+                    g.out[ty][a][r] = q.o;
+                }
+        }
+        s.has_grid = ok;
+        if (ok) s.grid = g;
+    }
     s.ns = ns;
     s.width = width;
     s.n2 = (int)o2.size();
@@ -323,6 +384,66 @@ static void lpt_schedule(const std::vector<BSTask> &tasks_in, const std::vector<
     toff[nt] = (int)packed.size();
 }
 
+// Z tiles of the twojmax-specialised kernel: kZTileA x kZTileB outputs of
+// one triple, scheduled over nt threads by longest processing time.  A tile
+// made only of the middle column's mirror rows (never read) is dropped.
+struct BSTile {
+    int t, a0, b0, na, nb;
+    long long cost;
+};
+
+static std::vector<BSTile> make_tiles(const std::set<int> &need, const std::vector<std::array<int, 4>> &trip) {
+    std::vector<BSTile> tiles;
+    for (int t : need) {
+        const int j1 = trip[t][0], j2 = trip[t][1], j = trip[t][2], nc = j / 2 + 1;
+        for (int a0 = 0; a0 <= j; a0 += kZTileA)
+            for (int b0 = 0; b0 < nc; b0 += kZTileB) {
+                const int na = std::min(kZTileA, j + 1 - a0), nb = std::min(kZTileB, nc - b0);
+                if (j % 2 == 0 && b0 == j / 2 && 2 * a0 > j) continue;
+                const int ca0 = (2 * a0 - j + j1 + j2) / 2, cb0 = (2 * b0 - j + j1 + j2) / 2;
+                const int nma1 = std::min(j1, ca0 + na - 1) - std::max(0, ca0 - j2) + 1;
+                const int nmb1 = std::min(j1, cb0 + nb - 1) - std::max(0, cb0 - j2) + 1;
+                const long long steps = (long long)std::max(nma1, 0) * std::max(nmb1, 0);
+                const long long cost = steps * (4 * kZTileA * kZTileB + 2 * kZTileA + 2 * kZTileB) +
+                                       (long long)std::max(nma1, 0) * (2 * kZTileA * kZTileB + 8) + 24;
+                tiles.push_back({t, a0, b0, na, nb, cost});
+            }
+    }
+    return tiles;
+}
+
+static void lpt_tiles(const std::vector<BSTile> &tiles_in, const std::vector<std::array<int, 4>> &trip,
+                      const std::vector<int> &cgoff, std::vector<int> &toff, std::vector<int4> &packed, int nt) {
+    std::vector<BSTile> tiles = tiles_in;
+    std::stable_sort(tiles.begin(), tiles.end(), [](const BSTile &a, const BSTile &b) { return a.cost > b.cost; });
+    std::vector<std::vector<BSTile>> bins(nt);
+    using E = std::pair<long long, int>;
+    std::priority_queue<E, std::vector<E>, std::greater<E>> heap;
+    for (int b = 0; b < nt; ++b) heap.push({0, b});
+    for (auto &tk : tiles) {
+        E e = heap.top();
+        heap.pop();
+        bins[e.second].push_back(tk);
+        e.first += tk.cost;
+        heap.push(e);
+    }
+    toff.assign(nt + 1, 0);
+    packed.clear();
+    for (int b = 0; b < nt; ++b) {
+        toff[b] = (int)packed.size();
+        for (auto &tk : bins[b]) {
+            const auto &tr = trip[tk.t];
+            int4 v;
+            v.x = tr[0] | (tr[1] << 8) | (tr[2] << 16) | (tk.a0 << 24);
+            v.y = tk.b0 | (tk.na << 8) | (tk.nb << 16);
+            v.z = tr[3];
+            v.w = cgoff[tk.t];
+            packed.push_back(v);
+        }
+    }
+    toff[nt] = (int)packed.size();
+}
+
 static int build_bs_impl(ld_descriptor *d, double rfac0, int J, int style, double rmin0, int switch_flag,
                          int bzero_flag, int ns, const double *cutoff, const double *weights);
 
@@ -393,6 +514,7 @@ static int build_bs_impl(ld_descriptor *d, double rfac0, int J, int style, doubl
             }
     b.ntrip = (int)trip.size();
     b.nZall = zoff;
+    b.ncg = (int)cg.size();
     std::vector<std::array<int, 3>> outs;
     bs_outputs(J, style, outs);
     b.ncoeff = (int)outs.size();
@@ -474,10 +596,10 @@ static int build_bs_impl(ld_descriptor *d, double rfac0, int J, int style, doubl
     {
         auto tf = make_tasks(need_f, d->bs_inner_fwd);
         lpt_schedule(tf, trip, cgoff, toff_f, task_f);
-        lpt_schedule(tf, trip, cgoff, toff2_f, task2_f, b.nt2);
+        lpt_tiles(make_tiles(need_f, trip), trip, cgoff, toff2_f, task2_f, b.nt2);
         auto tv = make_tasks(need_v, d->bs_inner_vjp);
         lpt_schedule(tv, trip, cgoff, toff_v, task_v);
-        lpt_schedule(tv, trip, cgoff, toff2_v, task2_v, b.nt2);
+        lpt_tiles(make_tiles(need_v, trip), trip, cgoff, toff2_v, task2_v, b.nt2);
         d->bs_tasks_fwd = (int)tf.size();
         d->bs_tasks_vjp = (int)tv.size();
     }
@@ -565,6 +687,7 @@ int launch_rows(ld_descriptor *d, const RowArgs &a0, cudaStream_t s) {
     a.pair_grid_mult = d->tune[LD_TUNE_PAIR_GRID_MULT];
     // the allocation-free entry point never takes the queue counter
     a.dynamic_queue = a0.fused_only ? 0 : d->tune[LD_TUNE_DYNAMIC_QUEUE];
+    a.force_generic = d->tune[LD_TUNE_SF_GENERIC] != 0;
     if (d->kind == LD_KIND_SYMMETRY_FUNCTIONS) return sf_launch(d->sf, a, s);
     return bs_launch(d->bs, a, s);
 }
@@ -1137,11 +1260,11 @@ int ld_gradient_rows_dev(ld_descriptor *d, int n_rows, const int *row_centre, co
 
 int ld_set_tuning(ld_descriptor *d, int key, int value) {
     if (!d) return fail(LD_ERR_INVALID_ARG, "descriptor handle is NULL");
-    if (key < 0 || key > LD_TUNE_DYNAMIC_QUEUE) return fail(LD_ERR_INVALID_ARG, "unknown tuning key");
+    if (key < 0 || key > LD_TUNE_SF_GENERIC) return fail(LD_ERR_INVALID_ARG, "unknown tuning key");
     if (value < 0) value = 0;
     if (key == LD_TUNE_SF_WARPS && value != 0 && value != 1 && value != 2 && value != 4)
         return fail(LD_ERR_INVALID_ARG, "LD_TUNE_SF_WARPS must be 1, 2 or 4");
-    if (key == LD_TUNE_DYNAMIC_QUEUE) value = value ? 1 : 0;
+    if (key == LD_TUNE_DYNAMIC_QUEUE || key == LD_TUNE_SF_GENERIC) value = value ? 1 : 0;
     std::lock_guard<std::mutex> lk(d->mu);
     d->tune[key] = value;
     return LD_OK;
@@ -1149,7 +1272,7 @@ int ld_set_tuning(ld_descriptor *d, int key, int value) {
 
 int ld_get_tuning(const ld_descriptor *d, int key, int *value) {
     if (!d || !value) return fail(LD_ERR_INVALID_ARG, "NULL argument");
-    if (key < 0 || key > LD_TUNE_DYNAMIC_QUEUE) return fail(LD_ERR_INVALID_ARG, "unknown tuning key");
+    if (key < 0 || key > LD_TUNE_SF_GENERIC) return fail(LD_ERR_INVALID_ARG, "unknown tuning key");
     *value = d->tune[key];
     return LD_OK;
 }

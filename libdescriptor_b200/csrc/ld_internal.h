@@ -47,6 +47,26 @@ struct DevBuf {
 // Device view of the parameter tables (outputs re-ordered for the kernel:
 // two-body outputs, then three-body outputs sorted by (type, eta) so that
 // consecutive outputs can share one exp()).
+// Factored form of a symmetry-function parameter set whose three-body
+// outputs of each type (g4, g5) lie on a grid of at most kSFGA angular terms
+// (lambda, zeta) x kSFGR radial terms (eta), with at most kSFG2 two-body
+// outputs.  Passed by value to the kernels (constant bank), so parameter
+// reads cost no memory instructions.
+constexpr int kSFGA = 4;
+constexpr int kSFGR = 4;
+constexpr int kSFG2 = 16;
+struct SFGrid {
+    int n2 = 0;
+    int t2[kSFG2] = {}, o2[kSFG2] = {};
+    double a2[kSFG2] = {}, b2[kSFG2] = {};
+    int na[2] = {0, 0}, nr[2] = {0, 0};            // [0]: g4, [1]: g5
+    double lam[2][kSFGA] = {}, zeta[2][kSFGA] = {}, P[2][kSFGA] = {};
+    int zi[2][kSFGA] = {};                          // integer zeta or -1
+    double eta[2][kSFGR] = {};                      // ascending
+    int ec[2][kSFGR] = {};                          // r > 0: k >= 2 -> E_0^k, else exp
+    int out[2][kSFGA][kSFGR] = {};                  // output index, -1: empty cell
+};
+
 struct SFDev {
     int ns = 0, width = 0;
     int n2 = 0, n3 = 0;
@@ -67,12 +87,14 @@ struct SFDev {
     // group base), k >= 2 the group base raised to the k-th power (eta is
     // k times the group's smallest eta)
     const int *ec3 = nullptr;
+    bool has_grid = false;
+    SFGrid grid;
 };
 
 // ------------------------------------------------------------- bispectrum
 struct BSDev {
     int J = 0, style = 3, switch_flag = 1, bzero_flag = 0, ns = 0;
-    int ncoeff = 0, nU = 0, nL = 0, ntrip = 0, nZall = 0;
+    int ncoeff = 0, nU = 0, nL = 0, ntrip = 0, nZall = 0, ncg = 0;
     double rfac0 = 0, rmin0 = 0, wself = 1.0;
     const double *rcut_flat = nullptr;  // per neighbour species (reference quirk)
     const double *wj = nullptr;         // per species weight
@@ -94,7 +116,9 @@ struct BSDev {
     const int4 *task_f = nullptr;
     const int *toff_v = nullptr;        // NT+1 (gradient: all needed triples)
     const int4 *task_v = nullptr;
-    // schedules of the twojmax-specialised per-centre kernel (nt2 threads)
+    // schedules of the twojmax-specialised per-centre kernel (nt2 threads):
+    // Z tiles packed as x = j1 | j2 << 8 | j << 16 | a0 << 24,
+    // y = b0 | rows << 8 | cols << 16, z = Z offset of the triple, w = CG offset
     int nt2 = 0;
     const int *toff2_f = nullptr;
     const int4 *task2_f = nullptr;
@@ -132,10 +156,26 @@ struct RowArgs {
     int ctas_per_sm = 0;               // per-centre bispectrum CTAs per SM
     int pair_grid_mult = 0;            // pair-parallel gradient grid = SMs x occupancy x this
     int dynamic_queue = 0;
+    bool force_generic = false;        // symmetry functions: table-driven kernel even when a grid exists
     // caller-provided device work space (nullable: stream-ordered allocation)
     void *work = nullptr;
     size_t work_bytes = 0;             // 1: rows claimed from an atomic counter instead of grid stride
 };
+
+// Z tiles of the twojmax-specialised per-centre kernel: one thread computes
+// kZTileA x kZTileB output elements (rows ma x columns mb) of one triple
+#ifndef LD_ZTILE_A
+#define LD_ZTILE_A 2
+#endif
+#ifndef LD_ZTILE_B
+#define LD_ZTILE_B 2
+#endif
+// 1: the Clebsch-Gordan table is copied to each CTA's shared memory
+#ifndef LD_CG_SHARED
+#define LD_CG_SHARED 1
+#endif
+constexpr int kZTileA = LD_ZTILE_A;
+constexpr int kZTileB = LD_ZTILE_B;
 
 // warps of the twojmax-specialised per-centre bispectrum CTA (4..8)
 constexpr int bs2_warps(int J) {
@@ -145,6 +185,7 @@ constexpr int bs2_warps(int J) {
 }
 
 int sf_launch(const SFDev &p, const RowArgs &a, cudaStream_t s);
+int sfg_launch(const SFDev &p, const RowArgs &a, cudaStream_t s);
 int bs_launch(const BSDev &p, const RowArgs &a, cudaStream_t s);
 size_t sf_work_bytes(const SFDev &p, int n_rows, bool vjp);
 size_t bs_work_bytes(const BSDev &p, int n_rows, bool vjp);

@@ -11,6 +11,8 @@
 #include <cstdint>
 #include <cstring>
 #include <string>
+#include <vector>
+#include <algorithm>
 
 #include "ld_internal.h"
 
@@ -67,19 +69,6 @@ extern "C" int ld_stage_request(int n_atoms, int n_total, long long nnz, int wid
     if (staging_bytes < L.total)
         return fail(LD_ERR_INVALID_ARG, "ld_stage_request: staging of " + std::to_string(staging_bytes) +
                                             " bytes < " + std::to_string(L.total) + " needed");
-    // validate the local indices before anything is written
-    long long sum = 0;
-    for (int j = 0; j < n_atoms; ++j) {
-        if (number_of_neighs[j] < 0) return fail(LD_ERR_INVALID_ARG, "negative neighbour count");
-        sum += number_of_neighs[j];
-    }
-    if (sum != nnz) return fail(LD_ERR_INVALID_ARG, "neighbour counts do not add up to nnz");
-    for (int g = 0; g < n_total; ++g)
-        if (image[g] < 0 || image[g] >= n_atoms) return fail(LD_ERR_INVALID_ARG, "image index outside the atoms");
-    for (long long e = 0; e < nnz; ++e)
-        if (neighbor_list[e] < 0 || neighbor_list[e] >= n_total)
-            return fail(LD_ERR_INVALID_ARG, "neighbour index outside the coordinates");
-
     char *b = static_cast<char *>(staging);
     double *s_coords = reinterpret_cast<double *>(b + L.off[0]);
     int *s_species = reinterpret_cast<int *>(b + L.off[1]);
@@ -89,18 +78,71 @@ extern "C" int ld_stage_request(int n_atoms, int n_total, long long nnz, int wid
     long long *s_begin = reinterpret_cast<long long *>(b + L.off[5]);
     int *s_counts = reinterpret_cast<int *>(b + L.off[6]);
     double *s_dE = reinterpret_cast<double *>(b + L.off[7]);
-    std::memcpy(s_coords, coords, (size_t)n_total * 24);
-    std::memcpy(s_species, species, (size_t)n_total * 4);
-    for (int g = 0; g < n_total; ++g) s_image[g] = image[g] + row0;
-    for (long long e = 0; e < nnz; ++e) s_nbl[e] = neighbor_list[e] + atom0;
+
+    // row arrays (sequential prefix) + count check
     long long pos = entry0;
     for (int j = 0; j < n_atoms; ++j) {
+        const int c = number_of_neighs[j];
+        if (c < 0) return fail(LD_ERR_INVALID_ARG, "negative neighbour count");
         s_centre[j] = atom0 + j;
         s_begin[j] = pos;
-        pos += number_of_neighs[j];
+        pos += c;
     }
-    std::memcpy(s_counts, number_of_neighs, (size_t)n_atoms * 4);
-    std::memcpy(s_dE, dE_ddesc, (size_t)n_atoms * width * 8);
+    if (pos - entry0 != nnz) return fail(LD_ERR_INVALID_ARG, "neighbour counts do not add up to nnz");
+
+    // bulk fields in chunks: plain copies and rebased index copies (with
+    // their range checks), spread over host threads for large requests
+    struct Job {
+        char *dst;
+        const char *src;
+        long long count;   // bytes (copy) or ints (rebase)
+        int add, hi;       // rebase: dst = src + add, src in [0, hi)
+        bool rebase;
+    };
+    Job jobs[6] = {
+        {(char *)s_coords, (const char *)coords, (long long)n_total * 24, 0, 0, false},
+        {(char *)s_species, (const char *)species, (long long)n_total * 4, 0, 0, false},
+        {(char *)s_counts, (const char *)number_of_neighs, (long long)n_atoms * 4, 0, 0, false},
+        {(char *)s_dE, (const char *)dE_ddesc, (long long)n_atoms * width * 8, 0, 0, false},
+        {(char *)s_image, (const char *)image, (long long)n_total, row0, n_atoms, true},
+        {(char *)s_nbl, (const char *)neighbor_list, nnz, atom0, n_total, true},
+    };
+    constexpr long long kChunkBytes = 1 << 20;
+    struct Piece {
+        int job;
+        long long lo, hi;
+    };
+    std::vector<Piece> pieces;
+    long long total = 0;
+    for (int k = 0; k < 6; ++k) {
+        const long long unit = jobs[k].rebase ? 4 : 1;
+        const long long step = kChunkBytes / unit;
+        for (long long lo = 0; lo < jobs[k].count; lo += step)
+            pieces.push_back({k, lo, std::min(jobs[k].count, lo + step)});
+        total += jobs[k].count * unit;
+    }
+    int bad = 0;
+    const int np = (int)pieces.size();
+    const int nthr = (int)std::max(1LL, std::min<long long>(8, total / (4 * kChunkBytes)));
+#pragma omp parallel for num_threads(nthr) schedule(dynamic, 1) reduction(| : bad) if (nthr > 1)
+    for (int i = 0; i < np; ++i) {
+        const Piece &pc = pieces[i];
+        const Job &jb = jobs[pc.job];
+        if (!jb.rebase) {
+            std::memcpy(jb.dst + pc.lo, jb.src + pc.lo, (size_t)(pc.hi - pc.lo));
+        } else {
+            const int *src = reinterpret_cast<const int *>(jb.src);
+            int *dst = reinterpret_cast<int *>(jb.dst);
+            int local_bad = 0;
+            for (long long e = pc.lo; e < pc.hi; ++e) {
+                const int v = src[e];
+                local_bad |= (v < 0) | (v >= jb.hi);
+                dst[e] = v + jb.add;
+            }
+            bad |= local_bad;
+        }
+    }
+    if (bad) return fail(LD_ERR_INVALID_ARG, "an image or neighbour index lies outside the request's atoms");
 
     cudaStream_t s = (cudaStream_t)stream;
     const auto h2d = cudaMemcpyHostToDevice;

@@ -17,63 +17,11 @@
 // type, assembles d/dr_j, d/dr_k, d/dr_i from them, accumulates neighbour
 // gradients in shared memory and scatters them with FP64 atomics (optionally
 // straight onto the ghost's master row).
-#include "ld_internal.h"
+#include "ld_sf_common.cuh"
 
 namespace ldb {
 namespace {
-
-constexpr double kPi = 3.1415926535897932;
-
-__device__ __forceinline__ void raise_status(int *status, int code) {
-    if (status) atomicCAS(status, 0, code);
-}
-
-__device__ __forceinline__ double cutc(double r, double rc) {
-    return (r < rc) ? 0.5 * (cos(kPi * r / rc) + 1.0) : 0.0;
-}
-__device__ __forceinline__ double dcutc(double r, double rc) {
-    return (r < rc) ? -0.5 * sin(kPi * r / rc) * (kPi / rc) : 0.0;
-}
-__device__ __forceinline__ double ipow(double x, int n) {
-    double r = 1.0;
-    for (int k = 0; k < n; ++k) r *= x;
-    return r;
-}
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
-struct WarpSlice {
-    double *cx, *cy, *cz, *r, *ir, *rc, *fc, *dfc, *gx, *gy, *gz;
-    int *spec, *idx, *inc;
-};
-
-__device__ __forceinline__ WarpSlice slice(double *base, int cap, bool vjp) {
-    WarpSlice s;
-    double *p = base;
-    s.cx = p; p += cap;
-    s.cy = p; p += cap;
-    s.cz = p; p += cap;
-    s.r = p; p += cap;
-    s.ir = p; p += cap;
-    s.rc = p; p += cap;
-    s.fc = p; p += cap;
-    if (vjp) {
-        s.dfc = p; p += cap;
-        s.gx = p; p += cap;
-        s.gy = p; p += cap;
-        s.gz = p; p += cap;
-    } else {
-        s.dfc = s.gx = s.gy = s.gz = nullptr;
-    }
-    int *q = reinterpret_cast<int *>(p);
-    s.spec = q; q += cap;
-    s.idx = q; q += cap;
-    s.inc = q;
-    return s;
-}
+using namespace sfc;
 
 template <bool VJP, int M2, int M3>
 __global__ void __launch_bounds__(kSFThreads, VJP ? 3 : 4)
@@ -388,50 +336,7 @@ sf_kernel(SFDev p, RowArgs a, int per_warp_doubles, int *queue) {
 
 template <bool VJP, int M2, int M3>
 int launch_t(const SFDev &p, const RowArgs &a, cudaStream_t s) {
-    const int cap = a.max_neigh > 0 ? a.max_neigh : 1;
-    const int ndbl = cap * (VJP ? 11 : 7);
-    const int per_warp = ndbl + (3 * cap + 1) / 2 + 2;  // doubles (ints packed after)
-    const size_t per_warp_bytes = (size_t)per_warp * sizeof(double);
-    int nw = (a.sf_warps == 1 || a.sf_warps == 2 || a.sf_warps == 4) ? a.sf_warps : 4;
-    while (nw > 1 && per_warp_bytes * nw > 200 * 1024) --nw;
-    if (per_warp_bytes * nw > 220 * 1024)
-        return fail(LD_ERR_CAPACITY, "symmetry functions: max_neigh=" + std::to_string(a.max_neigh) +
-                                         " exceeds the on-chip neighbour staging capacity");
-    const size_t smem = per_warp_bytes * nw;
-    auto kern = sf_kernel<VJP, M2, M3>;
-    LDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int dev = 0, nsm = 148, per_sm = 1;
-    LDB_CUDA(cudaGetDevice(&dev));
-    LDB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    LDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, nw * 32, smem));
-    if (per_sm < 1) per_sm = 1;
-    if (a.ctas_per_sm > 0 && a.ctas_per_sm < per_sm) per_sm = a.ctas_per_sm;
-    const int rows_per_block = nw;
-    long long want = (a.n_rows + rows_per_block - 1) / rows_per_block;
-    long long grid = (long long)nsm * per_sm;
-    if (want < grid) grid = want;
-    if (grid < 1) grid = 1;
-    int *queue = nullptr;
-    bool own = false;
-    if (a.dynamic_queue) {
-        if (a.work) {
-            if (a.work_bytes < sizeof(int)) return fail(LD_ERR_INVALID_ARG, "work space too small");
-            queue = static_cast<int *>(a.work);
-        } else {
-            LDB_CUDA(cudaMallocAsync((void **)&queue, sizeof(int), s));
-            own = true;
-        }
-        LDB_CUDA(cudaMemsetAsync(queue, 0, sizeof(int), s));
-    }
-    kern<<<(unsigned)grid, nw * 32, smem, s>>>(p, a, per_warp, queue);
-    count_launch();
-    cudaError_t e = cudaGetLastError();
-    if (own) {
-        cudaError_t e2 = cudaFreeAsync(queue, s);
-        if (e == cudaSuccess) e = e2;
-    }
-    if (e != cudaSuccess) return cuda_fail(e, "sf_kernel");
-    return LD_OK;
+    return launch_rows_kernel(sf_kernel<VJP, M2, M3>, p, a, s, VJP, "sf_kernel");
 }
 
 }  // namespace
@@ -440,6 +345,7 @@ size_t sf_work_bytes(const SFDev &, int, bool) { return 256; }
 
 int sf_launch(const SFDev &p, const RowArgs &a, cudaStream_t s) {
     if (a.n_rows <= 0) return LD_OK;
+    if (p.has_grid && !a.force_generic) return sfg_launch(p, a, s);
     const int m = p.n2 > p.n3 ? p.n2 : p.n3;
     const bool vjp = a.dE != nullptr;
     if (m <= 16) return vjp ? launch_t<true, 16, 16>(p, a, s) : launch_t<false, 16, 16>(p, a, s);

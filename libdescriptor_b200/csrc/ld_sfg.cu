@@ -1,0 +1,386 @@
+// ld_sfg.cu -- symmetry functions with a factored three-body parameter set.
+//
+// Same semantics as sf_kernel (SymmetryFunctions::compute,
+// src/SymmetryFunctions.cpp:141-259: g4 = 2^(1-zeta) sum (1 + lambda cos)^zeta
+// exp(-eta (r_ij^2 + r_ik^2 + r_jk^2)) fc fc fc, g5 without the r_jk terms).
+// When the three-body outputs of each type lie on a grid of angular terms
+// (lambda, zeta) x radial terms (eta) -- the usual Behler sets, e.g. 2 zeta x
+// 2 lambda x 4 eta -- a triplet needs only one power per angular term and one
+// exponential (or integer power of it) per radial term:
+//   acc(a, r) += cp_a * E_r * F,   output = 2^(1-zeta_a) * acc(a, r),
+// and the gradient's per-type sums A = sum g P cp E, B = sum g P cp eta E,
+// C = sum g P lambda dcp E factor the same way through
+//   s_a = sum_r gP(a, r) E_r,  t_a = sum_r gP(a, r) eta_r E_r.
+// Every parameter is a compile-time-indexed member of the by-value SFGrid,
+// so it is read from the constant bank; the upstream gradient of the row is
+// read once per centre into registers.
+#include "ld_sf_common.cuh"
+
+namespace ldb {
+namespace {
+using namespace sfc;
+
+constexpr int NA = kSFGA, NR = kSFGR;
+
+template <bool VJP, bool HAS4, bool HAS5>
+__global__ void __launch_bounds__(kSFThreads, VJP ? 3 : 4)
+sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue) {
+    extern __shared__ double smem[];
+    const SFGrid &g = p.grid;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int nw = blockDim.x >> 5;
+    const int cap = a.max_neigh;
+    WarpSlice S = slice(smem + (size_t)warp * per_warp, cap, VJP);
+    const int width = p.width;
+
+    int row = blockIdx.x * nw + warp;
+    if (queue) {
+        int r0 = 0;
+        if (lane == 0) r0 = atomicAdd(queue, 1);
+        row = __shfl_sync(0xffffffffu, r0, 0);
+    }
+    for (; row < a.n_rows;) {
+        const int i = a.row_centre ? a.row_centre[row] : row;
+        const int lrow = a.row_list ? a.row_list[row] : row;
+        const long long off = a.nbl_begin ? a.nbl_begin[lrow] : a.off[lrow];
+        const int n = (int)(a.off[lrow + 1] - a.off[lrow]);
+        const int cur_row = row;
+        if (queue) {
+            int r1 = 0;
+            if (lane == 0) r1 = atomicAdd(queue, 1);
+            row = __shfl_sync(0xffffffffu, r1, 0);
+        } else {
+            row += gridDim.x * nw;
+        }
+        double *const dco = VJP ? a.dcoords + (size_t)cur_row * a.dc_stride : nullptr;
+        if (n > cap || n < 0 || (a.n_total > 0 && (i < 0 || i >= a.n_total))) {
+            raise_status(a.status, n > cap ? kDevCapacity : kDevBadIndex);
+            if (a.desc)
+                for (int q = lane; q < width; q += 32)
+                    a.desc[(size_t)cur_row * width + q] = __longlong_as_double(0x7ff8000000000000LL);
+            continue;
+        }
+        const double cix = a.coords[3 * i], ciy = a.coords[3 * i + 1], ciz = a.coords[3 * i + 2];
+        const int is = a.species[i];
+        // ---- stage the neighbours of this row
+        for (int jj = lane; jj < n; jj += 32) {
+            int j = a.nbl[off + jj];
+            int ok = 1;
+            if (a.n_total > 0 && (j < 0 || j >= a.n_total)) {
+                raise_status(a.status, kDevBadIndex);
+                j = i;
+                ok = 0;
+            }
+            const int js = a.species[j];
+            const double x = a.coords[3 * j], y = a.coords[3 * j + 1], z = a.coords[3 * j + 2];
+            const double rx = x - cix, ry = y - ciy, rz = z - ciz;
+            const double r = sqrt(rx * rx + ry * ry + rz * rz);
+            const double rc = p.rcut[is * p.ns + js];
+            S.cx[jj] = x;
+            S.cy[jj] = y;
+            S.cz[jj] = z;
+            S.r[jj] = r;
+            S.ir[jj] = 1.0 / r;
+            S.rc[jj] = rc;
+            S.spec[jj] = js;
+            S.idx[jj] = ok ? j : -1;
+            S.inc[jj] = ok && !(r > rc);
+            S.fc[jj] = cutc(r, rc);
+            if (VJP) {
+                S.dfc[jj] = dcutc(r, rc);
+                S.gx[jj] = 0.0;
+                S.gy[jj] = 0.0;
+                S.gz[jj] = 0.0;
+            }
+        }
+        __syncwarp();
+        const double *dE = VJP ? a.dE + (size_t)cur_row * width : nullptr;
+        double gix = 0.0, giy = 0.0, giz = 0.0;
+        // ---- two-body terms
+        if (g.n2 > 0) {
+            double acc2[kSFG2];
+#pragma unroll
+            for (int q = 0; q < kSFG2; ++q) acc2[q] = 0.0;
+            double g2[kSFG2];
+            if (VJP) {
+#pragma unroll
+                for (int q = 0; q < kSFG2; ++q) g2[q] = q < g.n2 ? __ldg(dE + g.o2[q]) : 0.0;
+            }
+            for (int jj = lane; jj < n; jj += 32) {
+                if (!S.inc[jj]) continue;
+                const double r = S.r[jj], fc = S.fc[jj];
+                const double dfc = VJP ? S.dfc[jj] : 0.0;
+                double dsum = 0.0;
+#pragma unroll
+                for (int q = 0; q < kSFG2; ++q) {
+                    if (q < g.n2) {
+                        const int t = g.t2[q];
+                        const double pa = g.a2[q], pb = g.b2[q];
+                        double v, dv = 0.0;
+                        if (t == 1) {
+                            v = fc;
+                            if (VJP) dv = dfc;
+                        } else if (t == 2) {
+                            const double e = exp(-pa * (r - pb) * (r - pb));
+                            v = e * fc;
+                            if (VJP) dv = e * (-2.0 * pa * (r - pb) * fc + dfc);
+                        } else {
+                            double sn, cs;
+                            sincos(pa * r, &sn, &cs);
+                            v = cs * fc;
+                            if (VJP) dv = -pa * sn * fc + cs * dfc;
+                        }
+                        acc2[q] += v;
+                        if (VJP) dsum += g2[q] * dv;
+                    }
+                }
+                if (VJP) {
+                    const double inv = 1.0 / r;
+                    const double gx = dsum * (S.cx[jj] - cix) * inv;
+                    const double gy = dsum * (S.cy[jj] - ciy) * inv;
+                    const double gz = dsum * (S.cz[jj] - ciz) * inv;
+                    S.gx[jj] += gx;
+                    S.gy[jj] += gy;
+                    S.gz[jj] += gz;
+                    gix -= gx;
+                    giy -= gy;
+                    giz -= gz;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < kSFG2; ++q) {
+                if (q < g.n2) {
+                    const double v = warp_sum(acc2[q]);
+                    if (lane == 0 && a.desc) a.desc[(size_t)cur_row * width + g.o2[q]] = v;
+                }
+            }
+        }
+        // ---- three-body terms
+        if (HAS4 || HAS5) {
+            constexpr int NT = 2;
+            double acc[NT][NA][NR];
+            double gP[NT][NA][NR];
+#pragma unroll
+            for (int ty = 0; ty < NT; ++ty)
+#pragma unroll
+                for (int x = 0; x < NA; ++x)
+#pragma unroll
+                    for (int y = 0; y < NR; ++y) {
+                        const bool on = (ty == 0 ? HAS4 : HAS5);
+                        acc[ty][x][y] = 0.0;
+                        gP[ty][x][y] = 0.0;
+                        if (VJP && on && g.out[ty][x][y] >= 0)
+                            gP[ty][x][y] = __ldg(dE + g.out[ty][x][y]) * g.P[ty][x];
+                    }
+            int jj = 0, kk = 0;
+            {
+                int rem = lane;
+                while (jj < n - 1 && rem >= n - 1 - jj) {
+                    rem -= n - 1 - jj;
+                    ++jj;
+                }
+                kk = jj + 1 + rem;
+            }
+            while (jj < n - 1) {
+                if (S.inc[jj] && S.inc[kk]) {
+                    const int ks = S.spec[kk], js = S.spec[jj];
+                    const double rcjk = p.rcut[js * p.ns + ks];
+                    const double jkx = S.cx[kk] - S.cx[jj], jky = S.cy[kk] - S.cy[jj], jkz = S.cz[kk] - S.cz[jj];
+                    const double d = sqrt(jkx * jkx + jky * jky + jkz * jkz);
+                    const double av = S.r[jj], b = S.r[kk];
+                    const double ia = S.ir[jj], ib = S.ir[kk];
+                    const double asq = av * av, bsq = b * b, dsq = d * d;
+                    const double cth = (asq + bsq - dsq) * (0.5 * ia * ib);
+                    const double fa = S.fc[jj], fb = S.fc[kk];
+                    double fd = 0.0, dfd = 0.0;
+                    if (HAS4 && d < rcjk) {
+                        const double t = kPi * d / rcjk;
+                        if (VJP) {
+                            double sn, cs;
+                            sincos(t, &sn, &cs);
+                            fd = 0.5 * (cs + 1.0);
+                            dfd = -0.5 * sn * (kPi / rcjk);
+                        } else {
+                            fd = 0.5 * (cos(t) + 1.0);
+                        }
+                    }
+                    const bool g4ok = !(d > rcjk);
+                    double Aq[NT] = {0.0, 0.0}, Bq[NT] = {0.0, 0.0}, Cq[NT] = {0.0, 0.0};
+                    double Fq[NT];
+                    Fq[0] = fa * fb * fd;
+                    Fq[1] = fa * fb;
+#pragma unroll
+                    for (int ty = 0; ty < NT; ++ty) {
+                        if (!(ty == 0 ? HAS4 : HAS5)) continue;
+                        if (ty == 0 && !g4ok) continue;
+                        const double Ssum = ty == 0 ? asq + bsq + dsq : asq + bsq;
+                        // radial terms: one exp, integer multiples of the
+                        // smallest eta by binary powering
+                        double E[NR];
+#pragma unroll
+                        for (int y = 0; y < NR; ++y) {
+                            E[y] = 0.0;
+                            if (y < g.nr[ty]) {
+                                const int ec = g.ec[ty][y];
+                                if (y == 0 || ec < 2) {
+                                    E[y] = exp(-g.eta[ty][y] * Ssum);
+                                } else {
+                                    double rr = 1.0, xx = E[0];
+                                    for (int k = ec; k > 0; k >>= 1) {
+                                        if (k & 1) rr *= xx;
+                                        xx *= xx;
+                                    }
+                                    E[y] = rr;
+                                }
+                            }
+                        }
+                        // angular terms
+                        double cp[NA], dcp[NA];
+#pragma unroll
+                        for (int x = 0; x < NA; ++x) {
+                            cp[x] = 0.0;
+                            dcp[x] = 0.0;
+                            if (x < g.na[ty]) {
+                                const double base = 1.0 + g.lam[ty][x] * cth;
+                                if (base > 0) {
+                                    const int zi = g.zi[ty][x];
+                                    if (zi == 1) {
+                                        cp[x] = base;
+                                        dcp[x] = 1.0;
+                                    } else if (zi == 2) {
+                                        cp[x] = base * base;
+                                        dcp[x] = 2.0 * base;
+                                    } else if (zi == 4) {
+                                        const double b2 = base * base;
+                                        cp[x] = b2 * b2;
+                                        dcp[x] = 4.0 * b2 * base;
+                                    } else if (zi >= 0) {
+                                        cp[x] = ipow(base, zi);
+                                        dcp[x] = zi > 0 ? g.zeta[ty][x] * ipow(base, zi - 1) : 0.0;
+                                    } else {
+                                        cp[x] = pow(base, g.zeta[ty][x]);
+                                        dcp[x] = g.zeta[ty][x] * pow(base, g.zeta[ty][x] - 1.0);
+                                    }
+                                }
+                            }
+                        }
+                        const double F = Fq[ty];
+#pragma unroll
+                        for (int y = 0; y < NR; ++y) {
+                            const double W = E[y] * F;
+#pragma unroll
+                            for (int x = 0; x < NA; ++x) acc[ty][x][y] = fma(cp[x], W, acc[ty][x][y]);
+                        }
+                        if (VJP) {
+                            double Ee[NR];
+#pragma unroll
+                            for (int y = 0; y < NR; ++y) Ee[y] = g.eta[ty][y] * E[y];
+#pragma unroll
+                            for (int x = 0; x < NA; ++x) {
+                                double sa = 0.0, ta = 0.0;
+#pragma unroll
+                                for (int y = 0; y < NR; ++y) {
+                                    sa = fma(gP[ty][x][y], E[y], sa);
+                                    ta = fma(gP[ty][x][y], Ee[y], ta);
+                                }
+                                Aq[ty] = fma(cp[x], sa, Aq[ty]);
+                                Bq[ty] = fma(cp[x], ta, Bq[ty]);
+                                Cq[ty] = fma(g.lam[ty][x] * dcp[x], sa, Cq[ty]);
+                            }
+                        }
+                    }
+                    if (VJP) {
+                        const double F4 = Fq[0], F5 = Fq[1];
+                        const double A4 = Aq[0], B4 = Bq[0], C4 = Cq[0], A5 = Aq[1], B5 = Bq[1], C5 = Cq[1];
+                        const double dfa = S.dfc[jj], dfb = S.dfc[kk];
+                        const double dca = (asq - bsq + dsq) * (0.5 * ia * ia * ib);
+                        const double dcb = (bsq - asq + dsq) * (0.5 * ia * ib * ib);
+                        const double dcd = -d * ia * ib;
+                        const double Ga = F4 * C4 * dca - 2.0 * av * F4 * B4 + dfa * fb * fd * A4 +
+                                          F5 * C5 * dca - 2.0 * av * F5 * B5 + dfa * fb * A5;
+                        const double Gb = F4 * C4 * dcb - 2.0 * b * F4 * B4 + fa * dfb * fd * A4 +
+                                          F5 * C5 * dcb - 2.0 * b * F5 * B5 + fa * dfb * A5;
+                        const double Gd = F4 * C4 * dcd - 2.0 * d * F4 * B4 + fa * fb * dfd * A4 + F5 * C5 * dcd;
+                        const double id = d > 0 ? 1.0 / d : 0.0;
+                        const double ijx = (S.cx[jj] - cix) * ia, ijy = (S.cy[jj] - ciy) * ia,
+                                     ijz = (S.cz[jj] - ciz) * ia;
+                        const double ukx = (S.cx[kk] - cix) * ib, uky = (S.cy[kk] - ciy) * ib,
+                                     ukz = (S.cz[kk] - ciz) * ib;
+                        const double udx = jkx * id, udy = jky * id, udz = jkz * id;
+                        atomicAdd(&S.gx[jj], Ga * ijx - Gd * udx);
+                        atomicAdd(&S.gy[jj], Ga * ijy - Gd * udy);
+                        atomicAdd(&S.gz[jj], Ga * ijz - Gd * udz);
+                        atomicAdd(&S.gx[kk], Gb * ukx + Gd * udx);
+                        atomicAdd(&S.gy[kk], Gb * uky + Gd * udy);
+                        atomicAdd(&S.gz[kk], Gb * ukz + Gd * udz);
+                        gix -= Ga * ijx + Gb * ukx;
+                        giy -= Ga * ijy + Gb * uky;
+                        giz -= Ga * ijz + Gb * ukz;
+                    }
+                }
+                int rem = kk - (jj + 1) + 32;
+                while (jj < n - 1 && rem >= n - 1 - jj) {
+                    rem -= n - 1 - jj;
+                    ++jj;
+                }
+                kk = jj + 1 + rem;
+            }
+#pragma unroll
+            for (int ty = 0; ty < NT; ++ty)
+#pragma unroll
+                for (int x = 0; x < NA; ++x)
+#pragma unroll
+                    for (int y = 0; y < NR; ++y) {
+                        if ((ty == 0 ? HAS4 : HAS5) && g.out[ty][x][y] >= 0) {
+                            const double v = warp_sum(acc[ty][x][y]) * g.P[ty][x];
+                            if (lane == 0 && a.desc) a.desc[(size_t)cur_row * width + g.out[ty][x][y]] = v;
+                        }
+                    }
+        }
+        if (VJP) {
+            __syncwarp();
+            for (int jj = lane; jj < n; jj += 32) {
+                const int j = S.idx[jj];
+                if (j < 0) continue;
+                const int tj = a.image ? a.image[j] : j;
+                atomicAdd(dco + 3 * (size_t)tj, S.gx[jj]);
+                atomicAdd(dco + 3 * (size_t)tj + 1, S.gy[jj]);
+                atomicAdd(dco + 3 * (size_t)tj + 2, S.gz[jj]);
+            }
+            gix = warp_sum(gix);
+            giy = warp_sum(giy);
+            giz = warp_sum(giz);
+            if (lane == 0) {
+                const int ti = a.image ? a.image[i] : i;
+                atomicAdd(dco + 3 * (size_t)ti, gix);
+                atomicAdd(dco + 3 * (size_t)ti + 1, giy);
+                atomicAdd(dco + 3 * (size_t)ti + 2, giz);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+template <bool VJP, bool H4, bool H5>
+int launch_g(const SFDev &p, const RowArgs &a, cudaStream_t s) {
+    return launch_rows_kernel(sfg_kernel<VJP, H4, H5>, p, a, s, VJP, "sfg_kernel");
+}
+
+template <bool VJP>
+int launch_vjp(const SFDev &p, const RowArgs &a, cudaStream_t s) {
+    const bool h4 = p.grid.na[0] > 0, h5 = p.grid.na[1] > 0;
+    if (h4 && h5) return launch_g<VJP, true, true>(p, a, s);
+    if (h4) return launch_g<VJP, true, false>(p, a, s);
+    if (h5) return launch_g<VJP, false, true>(p, a, s);
+    return launch_g<VJP, false, false>(p, a, s);
+}
+
+}  // namespace
+
+int sfg_launch(const SFDev &p, const RowArgs &a, cudaStream_t s) {
+    if (a.n_rows <= 0) return LD_OK;
+    return a.dE ? launch_vjp<true>(p, a, s) : launch_vjp<false>(p, a, s);
+}
+
+}  // namespace ldb

@@ -89,6 +89,10 @@ class Abi:
                                                C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t,
                                                C.c_void_p]
             L.ld_rows_work_bytes.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_size_t)]
+            L.ld_stage_bytes.argtypes = [C.c_int, C.c_int, C.c_longlong, C.c_int, C.POINTER(C.c_size_t)]
+            L.ld_stage_request.argtypes = [C.c_int, C.c_int, C.c_longlong, C.c_int, C.c_int, C.c_int,
+                                           C.c_longlong, _dp, _ip, _ip, _ip, _ip, _dp, C.c_void_p, C.c_size_t]
+            L.ld_stage_request.argtypes += [C.c_void_p] * 9
             L.ld_set_tuning.argtypes = [C.c_void_p, C.c_int, C.c_int]
             L.ld_get_tuning.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
             cls._lib = L

@@ -228,3 +228,66 @@ def test_tuner_candidates_and_cache(tmp_path, monkeypatch):
     t2 = tuner.Autotuner(cache_path=path)
     monkeypatch.setattr(t2, "time_shape", lambda p, s: pytest.fail("timed a cached shape"))
     assert t2.tune(FakePass, "bs8", 1) == best_shape
+
+
+# ------------------------------------------------------- request staging
+def _stage(n, nt, nbl, counts, image, W=2, slots=(5, 100, 1000)):
+    import ctypes as C
+
+    from abi import Abi
+
+    L = Abi.lib()
+    rng = np.random.default_rng(2)
+    coords = rng.normal(size=(nt, 3))
+    species = (np.arange(nt) % 2).astype(np.int32)
+    dE = rng.normal(size=(n, W))
+    nb = C.c_size_t()
+    Abi.check(L.ld_stage_bytes(n, nt, len(nbl), W, C.byref(nb)))
+    raw = np.zeros(nb.value + 512, np.uint8)
+    base = (raw.ctypes.data + 255) & ~255
+    fake = [C.c_void_p(1 << 20)] * 8      # never dereferenced on the host
+    rc = L.ld_stage_request(n, nt, len(nbl), W, slots[0], slots[1], slots[2], np.ascontiguousarray(coords).ravel(),
+                            species, np.asarray(image, np.int32), np.asarray(nbl, np.int32),
+                            np.asarray(counts, np.int32), dE.ravel(), C.c_void_p(base), nb.value, *fake, None)
+    buf = raw[base - raw.ctypes.data:]
+    return rc, buf, coords, species, dE
+
+
+def test_stage_request_rebases_indices_into_staging():
+    """Host side of ld_stage_request: the staging layout holds the inputs
+    with indices rebased to the ring slots (the uploads need a device and
+    fail here with the no-device status, after the staging is written)."""
+    n, nt = 3, 5
+    counts = [2, 0, 3]
+    nbl = [1, 4, 0, 2, 3]
+    image = [0, 1, 2, 0, 2]
+    rc, buf, coords, species, dE = _stage(n, nt, nbl, counts, image)
+    assert rc != 0
+    up = lambda b: (b + 255) & ~255
+    sizes = [nt * 24, nt * 4, nt * 4, len(nbl) * 4, n * 4, n * 8, n * 4, n * 2 * 8]
+    offs = np.concatenate([[0], np.cumsum([up(s) for s in sizes])])
+    v = lambda i, dt, cnt: buf[offs[i]:offs[i] + cnt * np.dtype(dt).itemsize].view(dt)
+    np.testing.assert_array_equal(v(0, np.float64, 3 * nt), coords.ravel())
+    np.testing.assert_array_equal(v(1, np.int32, nt), species)
+    np.testing.assert_array_equal(v(2, np.int32, nt), np.asarray(image) + 5)
+    np.testing.assert_array_equal(v(3, np.int32, 5), np.asarray(nbl) + 100)
+    np.testing.assert_array_equal(v(4, np.int32, n), 100 + np.arange(n))
+    np.testing.assert_array_equal(v(5, np.int64, n), [1000, 1002, 1002])
+    np.testing.assert_array_equal(v(6, np.int32, n), counts)
+    np.testing.assert_array_equal(v(7, np.float64, 2 * n), dE.ravel())
+
+
+@pytest.mark.parametrize("bad", ["nbl", "image", "counts"])
+def test_stage_request_rejects_bad_indices(bad):
+    from abi import Abi
+
+    n, nt = 3, 5
+    counts, nbl, image = [2, 0, 3], [1, 4, 0, 2, 3], [0, 1, 2, 0, 2]
+    if bad == "nbl":
+        nbl = [1, 5, 0, 2, 3]          # 5 >= n_total
+    elif bad == "image":
+        image = [0, 1, 2, 3, 2]        # master 3 >= n_atoms
+    else:
+        counts = [2, 0, 2]             # does not add up to nnz
+    rc, *_ = _stage(n, nt, nbl, counts, image)
+    assert rc == 2, Abi.lib().ld_error_message().decode()   # LD_ERR_INVALID_ARG
