@@ -71,9 +71,10 @@ inline int per_warp_doubles(int cap, bool vjp) { return cap * (vjp ? 11 : 7) + (
 // tuned shape: warps per CTA (a.sf_warps), CTA cap per SM, optional dynamic
 // row queue (counter in the caller's work space or stream-ordered).
 template <class K, class P>
-int launch_rows_kernel(K kern, const P &p, const RowArgs &a, cudaStream_t s, bool vjp, const char *what) {
+int launch_rows_kernel(K kern, const P &p, const RowArgs &a, cudaStream_t s, bool vjp, const char *what,
+                       int extra_doubles = 0) {
     const int cap = a.max_neigh > 0 ? a.max_neigh : 1;
-    const int per_warp = per_warp_doubles(cap, vjp);
+    const int per_warp = per_warp_doubles(cap, vjp) + extra_doubles;
     const size_t per_warp_bytes = (size_t)per_warp * sizeof(double);
     int nw = (a.sf_warps == 1 || a.sf_warps == 2 || a.sf_warps == 4) ? a.sf_warps : 4;
     while (nw > 1 && per_warp_bytes * nw > 200 * 1024) --nw;

@@ -21,9 +21,18 @@ namespace {
 using namespace sfc;
 
 constexpr int NA = kSFGA, NR = kSFGR;
+// 1: the row's gP(a, r) = dL/dG * 2^(1-zeta) live in the warp's shared slice
+// (warp-uniform reads) instead of registers
+#ifndef LD_SFG_GP_SHARED
+#define LD_SFG_GP_SHARED 1
+#endif
+#ifndef LD_SFG_MINB
+#define LD_SFG_MINB 4
+#endif
+constexpr int kGPExtra = (LD_SFG_GP_SHARED ? 2 * NA * NR : 0);
 
 template <bool VJP, bool HAS4, bool HAS5>
-__global__ void __launch_bounds__(kSFThreads, VJP ? 3 : 4)
+__global__ void __launch_bounds__(kSFThreads, VJP ? LD_SFG_MINB : 4)
 sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue) {
     extern __shared__ double smem[];
     const SFGrid &g = p.grid;
@@ -160,7 +169,11 @@ sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue)
         if (HAS4 || HAS5) {
             constexpr int NT = 2;
             double acc[NT][NA][NR];
+#if LD_SFG_GP_SHARED
+            double(*gP)[NA][NR] = reinterpret_cast<double(*)[NA][NR]>(smem + (size_t)warp * per_warp + per_warp - kGPExtra);
+#else
             double gP[NT][NA][NR];
+#endif
 #pragma unroll
             for (int ty = 0; ty < NT; ++ty)
 #pragma unroll
@@ -169,10 +182,18 @@ sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue)
                     for (int y = 0; y < NR; ++y) {
                         const bool on = (ty == 0 ? HAS4 : HAS5);
                         acc[ty][x][y] = 0.0;
-                        gP[ty][x][y] = 0.0;
-                        if (VJP && on && g.out[ty][x][y] >= 0)
-                            gP[ty][x][y] = __ldg(dE + g.out[ty][x][y]) * g.P[ty][x];
+                        double v = 0.0;
+                        if (VJP && on && g.out[ty][x][y] >= 0) v = __ldg(dE + g.out[ty][x][y]) * g.P[ty][x];
+#if LD_SFG_GP_SHARED
+                        // the slice has room for gP only in the gradient kernel
+                        if (VJP && lane == 0) gP[ty][x][y] = v;
+#else
+                        gP[ty][x][y] = v;
+#endif
                     }
+#if LD_SFG_GP_SHARED
+            if (VJP) __syncwarp();
+#endif
             int jj = 0, kk = 0;
             {
                 int rem = lane;
@@ -364,7 +385,7 @@ sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue)
 
 template <bool VJP, bool H4, bool H5>
 int launch_g(const SFDev &p, const RowArgs &a, cudaStream_t s) {
-    return launch_rows_kernel(sfg_kernel<VJP, H4, H5>, p, a, s, VJP, "sfg_kernel");
+    return launch_rows_kernel(sfg_kernel<VJP, H4, H5>, p, a, s, VJP, "sfg_kernel", VJP ? kGPExtra : 0);
 }
 
 template <bool VJP>

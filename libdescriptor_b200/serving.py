@@ -232,10 +232,15 @@ class Scheduler:
         assert s == start
         ring.head = ring.live[-1][0] + ring.live[-1][1] if ring.live else 0
 
-    def admit(self, now: float) -> int:
+    def admit(self, now: float, max_rows: int | None = None) -> int:
+        """Admit pending requests in arrival order per lane while their
+        footprint fits; with ``max_rows``, stop a lane once that many rows
+        were staged in this call (so launches are not held back by a long
+        run of staging)."""
         n = 0
         for k, q in self.pending.items():
-            while q:
+            rows = 0
+            while q and (max_rows is None or rows < max_rows):
                 req = q[0]
                 if not self._try_admit(req):
                     self.admission_waits += 1
@@ -244,6 +249,7 @@ class Scheduler:
                 req.admitted_at = now
                 self.backend.stage(req)
                 self.admitted[k].append(req)
+                rows += req.n_atoms
                 n += 1
         return n
 
@@ -395,6 +401,7 @@ class ServingEngine:
                                out_rows=min(out_rows, min(c.rows for c in caps.values())))
         self.caps = caps
         self.launches = 0
+        self.host_stage_s = 0.0
         self.t0 = time.perf_counter()
 
     def clock(self) -> float:
@@ -413,6 +420,7 @@ class ServingEngine:
         ln = self.lanes[req.lane]
         r0, a0, e0 = req.slots
         n, nt, nnz, W = req.n_atoms, req.n_total, req.nnz, ln.W
+        t_in = time.perf_counter()
         nbytes = int(self._ext._stage_bytes(n, nt, nnz, W))
         units = max((nbytes + 255) // 256, 1)
         self._reclaim_staging(ln)
@@ -433,6 +441,7 @@ class ServingEngine:
         ev.record(ln.s_h2d)
         ln.staged.append((u0, ev))
         req.staged = ev
+        self.host_stage_s += time.perf_counter() - t_in
 
     def launch(self, plan: BatchPlan) -> None:
         torch = self.torch
@@ -480,7 +489,7 @@ class ServingEngine:
             self._ext._sync_status(ln.kind, ln.s_comp.cuda_stream)
 
     def serve(self, requests: list, arrivals: np.ndarray | None = None, keep_results: bool = False,
-              on_done=None) -> dict:
+              on_done=None, admit_rows: int = 1 << 16) -> dict:
         """Run an open-loop stream: request i is submitted at time
         arrivals[i] (seconds from the start; None: all at once).  Results
         are copied out of the output ring when ``keep_results`` (else only
@@ -488,6 +497,7 @@ class ServingEngine:
         order = np.argsort(arrivals, kind="stable") if arrivals is not None else np.arange(len(requests))
         arr = np.asarray(arrivals, dtype=np.float64) if arrivals is not None else np.zeros(len(requests))
         self.t0 = time.perf_counter()
+        self.host_stage_s = 0.0
         nxt = 0
         n = len(requests)
         done = 0
@@ -506,7 +516,7 @@ class ServingEngine:
                 if on_done is not None:
                     on_done(req)
                 done += 1
-            sched.admit(now)
+            sched.admit(now, admit_rows)
             sched.launch()
         self.torch.cuda.synchronize()
         self.check_status()
@@ -520,6 +530,7 @@ class ServingEngine:
                 "batches": sched.n_batches, "mean_batch_rows": float(np.mean(sched.batch_rows)) if sched.batch_rows else 0.0,
                 "max_batch_requests": int(max(sched.batch_reqs)) if sched.batch_reqs else 0,
                 "admission_waits": sched.admission_waits,
+                "host_staging_s": self.host_stage_s,
                 "gpu_launches": self.launches}
 
 
