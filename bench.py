@@ -41,6 +41,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "desc+VJP atoms/s, 1 B200: served batch vs plain call; p50/p99 ms @≤1e-10 rel"
+# DRAM bytes (read + write) per centre atom of the dominant kernels, from one
+# ncu capture each (profiles/): bispectrum 2J=8 pass (bsA + bsR, 8192-atom
+# launch: 5.03 MB + 21.98 MB) and the factored symmetry-function kernel
+# (4096-atom launch: 1.75 MB).  Traffic grows with the centres processed, so
+# other launch sizes are scaled by their atom counts.
+DRAM_BYTES_PER_ATOM = {"bs8": (5.027072e6 + 21.975296e6) / 8192, "sf24": 1.747968e6 / 4096}
 RATES = (1000.0, 10000.0, 50000.0)
 REQ_PER_STEP = 200
 MIX = {"sf": 0.7, "bs": 0.3}
@@ -376,15 +382,19 @@ def run_serve(args, torch, lds, dev, world, rank, local, dist):
     if rank != 0:
         return None
     bs_flops, sf_flops = flops_timed["bs"], flops_timed["sf"]
+    bs_atoms_timed = sum(sum(r.n_atoms for r in steps[i % len(steps)] if r.lane == "bs") for i in range(K))
     ach_bs = bs_flops / (ms["bs"] * 1e-3) / 1e12 if ms.get("bs") else 0.0
     ach_sf = sf_flops / (ms["sf"] * 1e-3) / 1e12 if ms.get("sf") else 0.0
     roof = {"bound": "fp64", "achieved": ach_bs, "peak": peak, "unit": "TFLOP/s", "frac": ach_bs / peak,
-            "traffic": None, "kernel": "bsA_kernel<8,1> + bsB_kernel<8> (bispectrum 2J=8 lane of the batched pass)",
+            "traffic": DRAM_BYTES_PER_ATOM["bs8"] * bs_atoms_timed / K,
+            "traffic_note": "bytes per step of the bispectrum lane, ncu DRAM bytes per atom of the 8192-atom "
+                            "launch (profiles/) times the lane's atoms per step",
+            "kernel": "bsA_kernel<8,1> + bsR_kernel<8> (bispectrum 2J=8 lane of the batched pass)",
             "flops_per_step": bs_flops / K, "share_of_pass_time": ms.get("bs", 0.0) / tot_ms,
             "peak_source": "bench.py FP64 FMA probe (ld_measure_fp64_peak), same run; MEASURED_PEAKS.json has no "
                            "FP64 figure",
             "call_weights_flops": {k: round(v, 1) for k, v in weights.items()},
-            "sf_lane": {"achieved": ach_sf, "frac": ach_sf / peak, "kernel": "sf_kernel<1,32,32>",
+            "sf_lane": {"achieved": ach_sf, "frac": ach_sf / peak, "kernel": "sfg_kernel<1,1,0>",
                         "share_of_pass_time": ms.get("sf", 0.0) / tot_ms}}
     cpu = None
     if not args.no_cpu_baseline and world == 1:
@@ -619,7 +629,9 @@ def run_single(args, torch, lds, dev, world, rank, local, dist):
     flop = algorithmic_flops(spec, cfg, weights)
     achieved = flop / (ms_per_step * 1e-3) / 1e12
     roof = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-            "traffic": None, "kernel": "bsA_kernel<8,1> + bsB_kernel<8>" if spec["kind"] == "bs" else "sf_kernel<1,32,32>",
+            "traffic": DRAM_BYTES_PER_ATOM[args.workload] * n,
+            "traffic_note": "ncu DRAM read + write bytes of one launch (profiles/)",
+            "kernel": "bsA_kernel<8,1> + bsR_kernel<8>" if spec["kind"] == "bs" else "sfg_kernel<1,1,0>",
             "flops_per_step": flop, "peak_source": "bench.py FP64 FMA probe (ld_measure_fp64_peak), same run",
             "call_weights_flops": {k: round(v, 1) for k, v in weights.items()},
             "hbm_bytes_per_step_algorithmic": int(cfg.coords.nbytes + cfg.nbl.nbytes + 8 * n * W * 2
