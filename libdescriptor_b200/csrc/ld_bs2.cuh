@@ -16,11 +16,15 @@
 // bsA_kernel<J, VJP>  one CTA per centre: stage neighbours, U (column lanes,
 //                     slots reduced through a per-warp buffer), Z (LPT task
 //                     lists), B; for the gradient also Y = sum betaj Z -> HBM.
-// bsB_kernel<J>       pair-parallel gradient: one slot per (centre, neighbour)
-//                     pair recomputes u and du/dr in registers and contracts
-//                     with the centre's Y on the fly: dL/dr_k = 2 w (dsfac
-//                     r_hat S + sfac V); FP64 atomics onto the neighbour and
-//                     the centre (or their master rows).
+// bsR_kernel<J>       pair-parallel gradient, reverse mode: one slot per
+//                     (centre, neighbour) pair runs the column recursion
+//                     forward (layer inputs kept in shared memory) and then
+//                     carries dPhi/du backward to dPhi/da, dPhi/db; chained to
+//                     the position with the Cayley-Klein derivatives, FP64
+//                     atomics onto the neighbour and the centre.
+// bsB_kernel<J>       the forward-mode form of the same gradient (u and the
+//                     three du/dr tangents carried together); kept for
+//                     comparison, built with LD_BS_REVERSE=0.
 #pragma once
 
 #include "ld_internal.h"
