@@ -278,6 +278,30 @@ int ld_build_neighbor_list(const double *coords, int n_total, double cutoff,
                            int *number_of_neighs, int *neighbor_list,
                            long long *nnz);
 
+/* Device forms of the two calls above (same ghosts in the same order with
+ * the same coordinates, and the same lists in the same order; every product
+ * and sum rounded as on the host).  coords, species, need_neigh and all
+ * outputs are device arrays; cell (9) and pbc (3) are host arrays.
+ *
+ * ld_create_paddings_dev: *n_pad receives the ghost count; with all of
+ * pad_coords / pad_species / pad_image NULL it only counts, otherwise it
+ * writes them (capacity max_pad ghosts, LD_ERR_CAPACITY beyond).
+ *
+ * ld_build_neighbor_list_dev: fills number_of_neighs[n_query] and the CSR
+ * offsets neigh_offsets[n_query+1] (the form ld_gradient_dev takes), and
+ * *nnz, *max_neigh (nullable); with neighbor_list NULL it stops there,
+ * otherwise it writes the list (capacity max_nnz, LD_ERR_CAPACITY beyond).
+ * Both wait for `stream` before returning (the counts are read back). */
+int ld_create_paddings_dev(double cutoff, const double *cell, const int *pbc,
+                           const double *coords, const int *species, int n_atoms,
+                           int max_pad, double *pad_coords, int *pad_species,
+                           int *pad_image, int *n_pad, ld_stream stream);
+int ld_build_neighbor_list_dev(const double *coords, int n_total, double cutoff,
+                               const int *need_neigh, int n_query,
+                               int *number_of_neighs, long long *neigh_offsets,
+                               long long max_nnz, int *neighbor_list,
+                               long long *nnz, int *max_neigh, ld_stream stream);
+
 /* ---------------- measurement helpers ------------------------------------- */
 
 /* Run `iters` rounds of FP64 fused multiply-adds on the device and report

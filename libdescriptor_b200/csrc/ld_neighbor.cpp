@@ -13,44 +13,19 @@
 #include <vector>
 
 #include "ld_internal.h"
+#include "ld_neighbor_math.h"
 
 namespace {
 
+using namespace ldnb;
 constexpr double kTol = 1.0e-10;
-
-inline double vdot(const double *a, const double *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
-inline double vnorm(const double *a) { return std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]); }
-inline void vcross(const double *a, const double *b, double *c) {
-    c[0] = a[1] * b[2] - a[2] * b[1];
-    c[1] = a[2] * b[0] - a[0] * b[2];
-    c[2] = a[0] * b[1] - a[1] * b[0];
-}
-inline double minor2(double a, double b, double c, double d) { return (a * d) - (b * c); }
-
-// inverse by cofactors / determinant; returns false when |det| < 1e-10
-bool invert3(const double *m, double *inv) {
-    inv[0] = minor2(m[4], m[5], m[7], m[8]);
-    inv[1] = minor2(m[2], m[1], m[8], m[7]);
-    inv[2] = minor2(m[1], m[2], m[4], m[5]);
-    inv[3] = minor2(m[5], m[3], m[8], m[6]);
-    inv[4] = minor2(m[0], m[2], m[6], m[8]);
-    inv[5] = minor2(m[2], m[0], m[5], m[3]);
-    inv[6] = minor2(m[3], m[4], m[6], m[7]);
-    inv[7] = minor2(m[1], m[0], m[7], m[6]);
-    inv[8] = minor2(m[0], m[1], m[3], m[4]);
-    const double det = m[0] * m[4] * m[8] - m[0] * m[5] * m[7] - m[1] * m[3] * m[8] + m[1] * m[5] * m[6] +
-                       m[2] * m[3] * m[7] - m[2] * m[4] * m[6];
-    if (std::abs(det) < kTol) return false;
-    for (int k = 0; k < 9; ++k) inv[k] /= det;
-    return true;
-}
 
 int paddings(double cutoff, const double *cell, const int *pbc, const double *x, const int *species, int n,
              std::vector<double> &pc, std::vector<int> &ps, std::vector<int> &pi) {
-    double tcell[9] = {cell[0], cell[3], cell[6], cell[1], cell[4], cell[7], cell[2], cell[5], cell[8]};
-    double fcell[9];
-    if (!invert3(tcell, fcell))
+    PadGeom g;
+    if (!pad_geometry(cutoff, cell, g))
         return ldb::fail(LD_ERR_INVALID_ARG, "In inverting the cell matrix, the determinant is 0!");
+    const double *tcell = g.tcell, *fcell = g.fcell;
     std::vector<double> frac((size_t)3 * n);
     double lo[3] = {1e10, 1e10, 1e10}, hi[3] = {-1e10, -1e10, -1e10};
     for (int a = 0; a < n; ++a) {
@@ -69,19 +44,8 @@ int paddings(double cutoff, const double *cell, const int *pbc, const double *x,
         lo[d] -= kTol;
         hi[d] += kTol;
     }
-    double xp[3];
-    vcross(cell + 3, cell + 6, xp);
-    const double volume = std::abs(vdot(cell, xp));
-    double dist[3];
-    vcross(cell + 3, cell + 6, xp);
-    dist[0] = volume / vnorm(xp);
-    vcross(cell + 6, cell + 0, xp);
-    dist[1] = volume / vnorm(xp);
-    vcross(cell, cell + 3, xp);
-    dist[2] = volume / vnorm(xp);
-    const double ratio[3] = {cutoff / dist[0], cutoff / dist[1], cutoff / dist[2]};
-    const int size[3] = {(int)std::ceil(ratio[0]), (int)std::ceil(ratio[1]), (int)std::ceil(ratio[2])};
-    const double slack[3] = {(double)size[0] - ratio[0], (double)size[1] - ratio[1], (double)size[2] - ratio[2]};
+    const int *size = g.size;
+    const double *slack = g.slack;
     for (int i = -size[0]; i <= size[0]; ++i)
         for (int j = -size[1]; j <= size[1]; ++j)
             for (int k = -size[2]; k <= size[2]; ++k) {

@@ -413,6 +413,33 @@ PYBIND11_MODULE(_libdescriptor, m) {
         }
         check(rc);
     });
+    m.def("_create_paddings_dev", [](double cutoff, DArr cell, IArr pbc, std::uintptr_t coords, std::uintptr_t species,
+                                     int n_atoms, int max_pad, std::uintptr_t pc, std::uintptr_t ps, std::uintptr_t pi,
+                                     std::uintptr_t stream) {
+        if (cell.size() != 9 || pbc.size() != 3) throw py::value_error("cell must have 9 values and pbc 3");
+        int n = 0, rc;
+        {
+            py::gil_scoped_release nogil;
+            rc = ld_create_paddings_dev(cutoff, cell.data(), pbc.data(), (const double *)coords, (const int *)species,
+                                        n_atoms, max_pad, (double *)pc, (int *)ps, (int *)pi, &n, (ld_stream)stream);
+        }
+        check(rc);
+        return n;
+    });
+    m.def("_build_neighbor_list_dev", [](std::uintptr_t coords, int n_total, double cutoff, std::uintptr_t need,
+                                         int n_query, std::uintptr_t counts, std::uintptr_t off, long long max_nnz,
+                                         std::uintptr_t nbl, std::uintptr_t stream) {
+        long long nnz = 0;
+        int mx = 0, rc;
+        {
+            py::gil_scoped_release nogil;
+            rc = ld_build_neighbor_list_dev((const double *)coords, n_total, cutoff, (const int *)need, n_query,
+                                            (int *)counts, (long long *)off, max_nnz, (int *)nbl, &nnz, &mx,
+                                            (ld_stream)stream);
+        }
+        check(rc);
+        return py::make_tuple(nnz, mx);
+    });
     m.def("_set_tuning", [](Kind &ds, int key, int value) { check(ld_set_tuning(ds.get(), key, value)); });
     m.def("_get_tuning", [](Kind &ds, int key) {
         int v = 0;

@@ -172,3 +172,60 @@ def fold(grad, n_atoms, image):
     out = np.array(grad[:n_atoms], dtype=np.float64, copy=True)
     np.add.at(out, image[n_atoms:], grad[n_atoms:])
     return out
+
+
+@dataclass
+class DeviceConfig:
+    """One configuration prepared on the device (``prepare_dev``): torch
+    tensors in the reference's layout plus the CSR row offsets."""
+
+    n_atoms: int
+    coords: object      # (n_total, 3) f64: contributing atoms, then ghosts
+    species: object     # (n_total,) i32
+    image: object       # (n_total,) i32
+    counts: object      # (n_atoms,) i32
+    off: object         # (n_atoms + 1,) i64
+    nbl: object         # (nnz,) i32
+    max_neigh: int
+
+    @property
+    def n_total(self) -> int:
+        return int(self.coords.shape[0])
+
+
+def prepare_dev(coords, cell, species, cutoff, pbc=(1, 1, 1), device="cuda", stream=None) -> DeviceConfig:
+    """``prepare`` on the device: ghost padding and the full neighbour list of
+    the contributing atoms with the library's device builder
+    (``ld_create_paddings_dev`` / ``ld_build_neighbor_list_dev``); the ghosts
+    and lists are identical to the host builder's."""
+    import torch
+
+    dev = torch.device(device)
+    s = stream if stream is not None else torch.cuda.current_stream(dev)
+    x = torch.as_tensor(np.ascontiguousarray(coords, dtype=np.float64), device=dev)
+    sp = torch.as_tensor(np.ascontiguousarray(species, dtype=np.int32), device=dev)
+    n = int(x.shape[0])
+    cellf = np.ascontiguousarray(cell, dtype=np.float64).reshape(9)
+    pbci = np.ascontiguousarray(pbc, dtype=np.int32)
+    m = _ext._create_paddings_dev(float(cutoff), cellf, pbci, x.data_ptr(), sp.data_ptr(), n, 0, 0, 0, 0,
+                                  s.cuda_stream)
+    allx = torch.empty((n + m, 3), dtype=torch.float64, device=dev)
+    alls = torch.empty(n + m, dtype=torch.int32, device=dev)
+    image = torch.empty(n + m, dtype=torch.int32, device=dev)
+    allx[:n] = x
+    alls[:n] = sp
+    image[:n] = torch.arange(n, dtype=torch.int32, device=dev)
+    if m:
+        _ext._create_paddings_dev(float(cutoff), cellf, pbci, x.data_ptr(), sp.data_ptr(), n, m,
+                                  allx[n:].data_ptr(), alls[n:].data_ptr(), image[n:].data_ptr(), s.cuda_stream)
+    need = torch.zeros(n + m, dtype=torch.int32, device=dev)
+    need[:n] = 1
+    counts = torch.empty(n, dtype=torch.int32, device=dev)
+    off = torch.empty(n + 1, dtype=torch.int64, device=dev)
+    nnz, _ = _ext._build_neighbor_list_dev(allx.data_ptr(), n + m, float(cutoff), need.data_ptr(), n,
+                                           counts.data_ptr(), off.data_ptr(), 0, 0, s.cuda_stream)
+    nbl = torch.empty(max(int(nnz), 1), dtype=torch.int32, device=dev)
+    nnz, mx = _ext._build_neighbor_list_dev(allx.data_ptr(), n + m, float(cutoff), need.data_ptr(), n,
+                                            counts.data_ptr(), off.data_ptr(), int(nnz), nbl.data_ptr(),
+                                            s.cuda_stream)
+    return DeviceConfig(n, allx, alls, image, counts, off, nbl[:int(nnz)], max(int(mx), 1))
