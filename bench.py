@@ -41,6 +41,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "desc+VJP atoms/s, 1 B200: served batch vs plain call; p50/p99 ms @≤1e-10 rel"
+from libdescriptor_b200.replicas import replica_throughput  # noqa: E402
 # DRAM bytes (read + write) per centre atom of the dominant kernels, from one
 # ncu capture each (profiles/): bispectrum 2J=8 pass (bsA + bsR, 8192-atom
 # launch: 5.03 MB + 21.98 MB) and the factored symmetry-function kernel
@@ -342,15 +343,10 @@ def run_serve(args, torch, lds, dev, world, rank, local, dist):
         for ps, _ in passes[0].values():
             ps.sync_status()
         ms = {k: sum(a.elapsed_time(b) for a, b in v) for k, v in evs.items()}
-        tot_ms = sum(ms.values())
-        if dist:
-            t = torch.tensor([tot_ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            tot_ms = float(t.item())
         step_atoms = [sum(r.n_atoms for r in st) for st in steps]
         atoms_timed = sum(step_atoms[i % len(steps)] for i in range(K))
         atoms_total = sum(r.n_atoms for r in reqs)
-        value = world * atoms_timed / (tot_ms * 1e-3)
+        value, tot_ms, _ = replica_throughput(atoms_timed, sum(ms.values()), dist, dev)
         flops_timed = {k: sum(per[k][1] for i in range(K) for per in [passes[i % len(passes)]] if k in per)
                        for k in kinds}
         del passes
@@ -487,12 +483,7 @@ def run_batch512(args, torch, lds, dev, world, rank, local, dist):
     # graph replays: count kernels per captured pass
     launches = sum(ps.launches_per_pass for ps in passes.values()) * args.steps
     ms = {k: sum(a.elapsed_time(b_) for a, b_ in v) / args.steps for k, v in evs.items()}
-    step_ms = sum(ms.values())
-    if dist:
-        t = torch.tensor([step_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        step_ms = float(t.item())
-    value = world * n_rows / (step_ms * 1e-3)
+    value, step_ms, _ = replica_throughput(n_rows, sum(ms.values()), dist, dev)
     # e2e: the same 512 cells x 2 descriptors as requests to the server, host in/out
     reqs = []
     rng = np.random.default_rng(5)
@@ -605,12 +596,8 @@ def run_single(args, torch, lds, dev, world, rank, local, dist):
     launches = lds.launch_count() - l0
     lds._ext._sync_status(ds, s)
     tot_ms = float(sum(a.elapsed_time(b) for a, b in evs))
-    if dist:
-        t = torch.tensor([tot_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_ms = float(t.item())
+    value, tot_ms, _ = replica_throughput(n * args.steps, tot_ms, dist, dev)
     ms_per_step = tot_ms / args.steps
-    value = world * n / (ms_per_step * 1e-3)
     for _ in range(2):
         lds.compute_and_gradient(ds, n, cfg.species, cfg.nbl, cfg.counts, cfg.coords, dE_h)
     torch.cuda.synchronize()
