@@ -515,6 +515,21 @@ static int build_bs_impl(ld_descriptor *d, double rfac0, int J, int style, doubl
     b.ntrip = (int)trip.size();
     b.nZall = zoff;
     b.ncg = (int)cg.size();
+    // anti-diagonal packing: for output m of triple (j1, j2, j) the valid
+    // entries are m1 + m2 = c + m, c = (j1 + j2 - j) / 2, m1 in
+    // [max(0, c + m - j2), min(j1, c + m)]
+    std::vector<double> cgp;
+    std::vector<int> dbase, doffs;
+    for (size_t t = 0; t < trip.size(); ++t) {
+        const int j1 = trip[t][0], j2 = trip[t][1], j = trip[t][2], c = (j1 + j2 - j) / 2;
+        doffs.push_back((int)dbase.size());
+        for (int m = 0; m <= j; ++m) {
+            const int sd = c + m, lo = std::max(0, sd - j2), hi = std::min(j1, sd);
+            dbase.push_back((int)cgp.size() - lo);
+            for (int m1 = lo; m1 <= hi; ++m1) cgp.push_back(cg[cgoff[t] + m1 * (j2 + 1) + (sd - m1)]);
+        }
+    }
+    b.ncgp = (int)cgp.size();
     std::vector<std::array<int, 3>> outs;
     bs_outputs(J, style, outs);
     b.ncoeff = (int)outs.size();
@@ -596,10 +611,10 @@ static int build_bs_impl(ld_descriptor *d, double rfac0, int J, int style, doubl
     {
         auto tf = make_tasks(need_f, d->bs_inner_fwd);
         lpt_schedule(tf, trip, cgoff, toff_f, task_f);
-        lpt_tiles(make_tiles(need_f, trip), trip, cgoff, toff2_f, task2_f, b.nt2);
+        lpt_tiles(make_tiles(need_f, trip), trip, doffs, toff2_f, task2_f, b.nt2);
         auto tv = make_tasks(need_v, d->bs_inner_vjp);
         lpt_schedule(tv, trip, cgoff, toff_v, task_v);
-        lpt_tiles(make_tiles(need_v, trip), trip, cgoff, toff2_v, task2_v, b.nt2);
+        lpt_tiles(make_tiles(need_v, trip), trip, doffs, toff2_v, task2_v, b.nt2);
         d->bs_tasks_fwd = (int)tf.size();
         d->bs_tasks_vjp = (int)tv.size();
     }
@@ -614,6 +629,8 @@ static int build_bs_impl(ld_descriptor *d, double rfac0, int J, int style, doubl
     ar.add(lblock, &b.lblock);
     ar.add(trip4, &b.trip);
     ar.add(cgoff, &b.cgoff);
+    ar.add(cgp, &b.cgp);
+    ar.add(dbase, &b.dbase);
     ar.add(cg, &b.cg);
     ar.add(otrip, &b.otrip);
     ar.add(moff, &b.moff);

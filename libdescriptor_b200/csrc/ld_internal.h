@@ -105,6 +105,12 @@ struct BSDev {
     const int4 *trip = nullptr;         // (j1, j2, j, zoff)
     const int *cgoff = nullptr;         // per triple
     const double *cg = nullptr;
+    // CG blocks packed by anti-diagonal m1 + m2 (the entries with a valid
+    // output index only) for the tiled Z: entry (m1, output m) of triple t is
+    // cgp[dbase[tri_off(t) + m] + m1]
+    int ncgp = 0;
+    const double *cgp = nullptr;
+    const int *dbase = nullptr;
     const int *otrip = nullptr;         // per output: triple index
     const int *moff = nullptr;          // per triple CSR into (mo, mcoef)
     const int *mo = nullptr;
@@ -118,7 +124,8 @@ struct BSDev {
     const int4 *task_v = nullptr;
     // schedules of the twojmax-specialised per-centre kernel (nt2 threads):
     // Z tiles packed as x = j1 | j2 << 8 | j << 16 | a0 << 24,
-    // y = b0 | rows << 8 | cols << 16, z = Z offset of the triple, w = CG offset
+    // y = b0 | rows << 8 | cols << 16, z = Z offset of the triple,
+    // w = the triple's first entry in dbase
     int nt2 = 0;
     const int *toff2_f = nullptr;
     const int4 *task2_f = nullptr;
