@@ -38,7 +38,7 @@ __host__ __device__ constexpr int ncols(int J) { return J / 2 + 1; }
 __host__ __device__ constexpr int slots_per_warp(int J) { return 32 / ncols(J); }
 // left-half layer offset: sum_{j'<j} (j'+1)(j'/2+1)
 __host__ __device__ constexpr int lblock(int j) { return j <= 0 ? 0 : lblock(j - 1) + j * ((j - 1) / 2 + 1); }
-// warps of the per-centre CTA: enough slots for ~36 neighbours, 4..8 warps
+// warps of the per-centre CTA: enough slots for ~32 neighbours, 4..8 warps
 __host__ __device__ constexpr int warpsA(int J) { return bs2_warps(J); }
 
 __device__ __forceinline__ void raise_status(int *status, int code) {

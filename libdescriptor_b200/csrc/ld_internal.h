@@ -184,11 +184,16 @@ struct RowArgs {
 constexpr int kZTileA = LD_ZTILE_A;
 constexpr int kZTileB = LD_ZTILE_B;
 
-// warps of the twojmax-specialised per-centre bispectrum CTA (4..8)
+// warps of the twojmax-specialised per-centre bispectrum CTA (4..8): enough
+// neighbour slots for about 32 neighbours in one round
+#ifndef LD_BS2_WARPS
+#define LD_BS2_WARPS 0
+#endif
 constexpr int bs2_warps(int J) {
-    return (36 + 32 / (J / 2 + 1) - 1) / (32 / (J / 2 + 1)) < 4   ? 4
-           : (36 + 32 / (J / 2 + 1) - 1) / (32 / (J / 2 + 1)) > 8 ? 8
-                                                                  : (36 + 32 / (J / 2 + 1) - 1) / (32 / (J / 2 + 1));
+    return LD_BS2_WARPS > 0 ? LD_BS2_WARPS
+           : (32 + 32 / (J / 2 + 1) - 1) / (32 / (J / 2 + 1)) < 4 ? 4
+           : (32 + 32 / (J / 2 + 1) - 1) / (32 / (J / 2 + 1)) > 8 ? 8
+                                                                  : (32 + 32 / (J / 2 + 1) - 1) / (32 / (J / 2 + 1));
 }
 
 int sf_launch(const SFDev &p, const RowArgs &a, cudaStream_t s);
