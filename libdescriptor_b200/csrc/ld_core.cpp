@@ -126,7 +126,7 @@ struct ld_descriptor {
     ldb::BSDev bs;
     ldb::DevBuf tables;
     // host-API staging (grow-only)
-    ldb::DevBuf species, nbl, off, coords, desc, dE, dc, centre, list, status, tmp;
+    ldb::DevBuf species, nbl, off, coords, desc, dE, dc, centre, list, status, tmp, work;
     cudaStream_t stream = nullptr;
     std::mutex mu;
     // introspection
@@ -828,7 +828,16 @@ static int host_pass_impl(ld_descriptor *d, HostRows &h, int n_total, const int 
         a.dcoords = d->dc.as<double>();
         if (jac_width > 0) a.desc = nullptr;
     }
-    if (rows > 0 && (rc = launch_rows(d, a, s))) return rc;
+    if (rows > 0) {
+        // the kernels' work space lives in a grow-only buffer of the handle,
+        // so repeated calls allocate nothing
+        size_t wb = 0;
+        if ((rc = ld_rows_work_bytes(d, rows, dE ? 1 : 0, &wb))) return rc;
+        if ((rc = d->work.ensure(wb))) return rc;
+        a.work = d->work.p;
+        a.work_bytes = wb;
+        if ((rc = launch_rows(d, a, s))) return rc;
+    }
     if (dE) {
         const size_t ndc = jac_width > 0 ? (size_t)rows * 3 * n_total : (size_t)3 * n_total;
         LDB_CUDA(cudaMemcpyAsync(dcoords, d->dc.p, sizeof(double) * ndc, cudaMemcpyDeviceToHost, s));
