@@ -611,8 +611,11 @@ static int bs2_dispatch(const BSDev &p, const RowArgs &a, cudaStream_t s) {
 }
 
 size_t bs_work_bytes(const BSDev &p, int n_rows, bool vjp) {
-    const size_t y = vjp ? ((sizeof(double2) * (size_t)(n_rows > 0 ? n_rows : 0) * p.nL + 16 + 255) & ~(size_t)255) : 0;
-    return y + 256;
+    const size_t rows = (size_t)(n_rows > 0 ? n_rows : 0);
+    const size_t y = vjp ? ((sizeof(double2) * rows * p.nL + 16 + 255) & ~(size_t)255) : 0;
+    // the split form's U blocks: [group of 32 rows][element][row % 32]
+    const size_t ug = bs_split(p) ? ((((rows + 31) / 32) * p.nU * 32 * sizeof(double2) + 255) & ~(size_t)255) : 0;
+    return y + ug + 256;
 }
 
 int bs_launch(const BSDev &p, const RowArgs &a, cudaStream_t s) {

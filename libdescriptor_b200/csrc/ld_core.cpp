@@ -618,6 +618,80 @@ static int build_bs_impl(ld_descriptor *d, double rfac0, int J, int style, doubl
         d->bs_tasks_fwd = (int)tf.size();
         d->bs_tasks_vjp = (int)tv.size();
     }
+    // rows-in-lanes Z schedule: one item per output row (j, ma) of a layer
+    // with needed triples; its cost counts the window steps of every triple
+    // of the layer; items go to the least loaded warp, largest first
+    std::vector<int> oslot(outs.size(), -1), tslot(trip.size(), -1);
+    b.nbslot = 0;
+    for (size_t o = 0; o < outs.size(); ++o) {
+        const int t = otrip[o];
+        if (t < 0) continue;
+        if (tslot[t] < 0) tslot[t] = b.nbslot++;
+        oslot[o] = tslot[t];
+    }
+    // column weights by window step: G_t[mb][q] = cg(c + q - mb, mb)
+    std::vector<double> zg;
+    std::vector<int> gofs(trip.size(), 0);
+    for (size_t t = 0; t < trip.size(); ++t) {
+        const int j1 = trip[t][0], j2 = trip[t][1], j = trip[t][2], c = (j1 + j2 - j) / 2;
+        const int nc = j / 2 + 1, ncp = nc + (nc & 1), nst = std::min(j2, c + nc - 1) + 1;
+        gofs[t] = (int)zg.size();
+        for (int mb = 0; mb < nst; ++mb)
+            for (int q = 0; q < ncp; ++q) {
+                const int mb1 = c + q - mb;
+                zg.push_back(q < nc && mb1 >= 0 && mb1 <= j1 ? cg[cgoff[t] + mb1 * (j2 + 1) + mb] : 0.0);
+            }
+    }
+    auto zsched = [&](const std::set<int> &need, std::vector<int> &zoff, std::vector<int> &zitem,
+                      std::vector<int> &ztoff, std::vector<int4> &ztl) {
+        ztoff.assign(J + 2, 0);
+        ztl.clear();
+        std::vector<std::pair<long long, int>> items;
+        for (int j = 0; j <= J; ++j) {
+            ztoff[j] = (int)ztl.size();
+            const int nc = j / 2 + 1;
+            for (int t : need) {
+                if (trip[t][2] != j) continue;
+                const int j1 = trip[t][0], j2 = trip[t][1], c = (j1 + j2 - j) / 2;
+                ztl.push_back(make_int4(j1 | (j2 << 8) | (c << 16), gofs[t], cgoff[t], t | ((tslot[t] + 1) << 16)));
+            }
+            const int t0 = ztoff[j], t1 = (int)ztl.size();
+            if (t1 == t0) continue;
+            for (int ma = 0; ma <= j; ++ma) {
+                long long cost = 16;
+                for (int k = t0; k < t1; ++k) {
+                    const int j1 = ztl[k].x & 0xff, j2 = (ztl[k].x >> 8) & 0xff, c = (ztl[k].x >> 16) & 0xff;
+                    const int rows = std::min(j2, c + ma) - std::max(0, c + ma - j1) + 1;
+                    const int steps = std::min(j2, c + nc - 1) + 1;
+                    cost += (long long)rows * (steps * (6 * nc + 6) + 4 * nc + 16) + 8 * nc + 32;
+                }
+                items.push_back({cost, j | (ma << 8)});
+            }
+        }
+        ztoff[J + 1] = (int)ztl.size();
+        std::stable_sort(items.begin(), items.end(),
+                         [](const std::pair<long long, int> &x, const std::pair<long long, int> &y) {
+                             return x.first > y.first;
+                         });
+        std::vector<std::vector<int>> bins(kZWarps);
+        std::vector<long long> load(kZWarps, 0);
+        for (auto &it : items) {
+            const int w = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+            bins[w].push_back(it.second);
+            load[w] += it.first;
+        }
+        zoff.assign(kZWarps + 1, 0);
+        zitem.clear();
+        for (int w = 0; w < kZWarps; ++w) {
+            zoff[w] = (int)zitem.size();
+            zitem.insert(zitem.end(), bins[w].begin(), bins[w].end());
+        }
+        zoff[kZWarps] = (int)zitem.size();
+    };
+    std::vector<int> zoff_f, zitem_f, ztoff_f, zoff_v, zitem_v, ztoff_v;
+    std::vector<int4> ztl_f, ztl_v;
+    zsched(need_f, zoff_f, zitem_f, ztoff_f, ztl_f);
+    zsched(need_v, zoff_v, zitem_v, ztoff_v, ztl_v);
     std::vector<int4> trip4;
     for (auto &t : trip) trip4.push_back(make_int4(t[0], t[1], t[2], t[3]));
     Arena ar;
@@ -647,6 +721,16 @@ static int build_bs_impl(ld_descriptor *d, double rfac0, int J, int style, doubl
     ar.add(task2_f, &b.task2_f);
     ar.add(toff2_v, &b.toff2_v);
     ar.add(task2_v, &b.task2_v);
+    ar.add(oslot, &b.oslot);
+    ar.add(zg, &b.zg);
+    ar.add(zoff_f, &b.zoff_f);
+    ar.add(zitem_f, &b.zitem_f);
+    ar.add(ztoff_f, &b.ztoff_f);
+    ar.add(ztl_f, &b.ztl_f);
+    ar.add(zoff_v, &b.zoff_v);
+    ar.add(zitem_v, &b.zitem_v);
+    ar.add(ztoff_v, &b.ztoff_v);
+    ar.add(ztl_v, &b.ztl_v);
     int rc = ar.upload(d->tables);
     if (rc) return rc;
     d->kind = LD_KIND_BISPECTRUM;

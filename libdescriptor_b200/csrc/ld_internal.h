@@ -131,6 +131,23 @@ struct BSDev {
     const int4 *task2_f = nullptr;
     const int *toff2_v = nullptr;
     const int4 *task2_v = nullptr;
+    // rows-in-lanes Z kernel (kZWarps warps, one row per lane): items
+    // (j | ma << 8), one output row of layer j each, scheduled per warp
+    // (zoff: kZWarps+1); the triples of layer j are ztl[ztoff[j] ..
+    // ztoff[j+1]) packed as x = j1 | j2 << 8 | c << 16 (c = (j1+j2-j)/2),
+    // y = offset of its column weights in zg, z = cgoff of the triple,
+    // w = triple index | (descriptor slot + 1) << 16 (slot -1: no output);
+    // oslot maps an output to its slot
+    int nbslot = 0;
+    const int *oslot = nullptr;
+    // per triple: its column weights by window step, G[mb][q] = cg(c + q -
+    // mb, mb) (zero outside the triple's range), q padded to even, at zg +
+    // the triple's ztl y field
+    const double *zg = nullptr;
+    const int *zoff_f = nullptr, *zitem_f = nullptr, *ztoff_f = nullptr;
+    const int4 *ztl_f = nullptr;
+    const int *zoff_v = nullptr, *zitem_v = nullptr, *ztoff_v = nullptr;
+    const int4 *ztl_v = nullptr;
 };
 
 constexpr int kBSThreads = 128;   // threads per bispectrum CTA (one centre)
@@ -183,6 +200,28 @@ struct RowArgs {
 #endif
 constexpr int kZTileA = LD_ZTILE_A;
 constexpr int kZTileB = LD_ZTILE_B;
+
+// 1: the twojmax-specialised path runs U (per centre), Z/B/Y (rows in
+// lanes) and the pair gradient as three kernels; 0: the per-centre kernel
+// computes U, Z, B and Y together
+#ifndef LD_BS_SPLIT
+#define LD_BS_SPLIT 1
+#endif
+// warps of the rows-in-lanes Z kernel's CTA (32 rows per CTA)
+#ifndef LD_ZWARPS
+#define LD_ZWARPS 16
+#endif
+constexpr int kZWarps = LD_ZWARPS;
+// shared memory of the rows-in-lanes Z kernel: the 32 rows' full U
+// ([element][lane], 512 bytes per element) between zero guards of J+1
+// elements before and J/2+1 after (reads just outside a row land there or
+// in other elements of the lane, always finite, and meet a zero weight),
+// then the descriptor sums [lane][slot]
+inline size_t bs_smemZ_bytes(const BSDev &p) {
+    return (size_t)(p.J + 1 + p.nU + p.J / 2 + 1) * 32 * 16 + (size_t)32 * (p.nbslot > 0 ? p.nbslot : 1) * 8;
+}
+// the split form runs where its Z kernel fits one SM's shared memory
+inline bool bs_split(const BSDev &p) { return LD_BS_SPLIT != 0 && bs_smemZ_bytes(p) <= 227 * 1024; }
 
 // warps of the twojmax-specialised per-centre bispectrum CTA (4..8): enough
 // neighbour slots for about 32 neighbours in one round

@@ -51,7 +51,7 @@ def test_burst_with_admission_waits_matches_alone(stream_setup):
 
     kinds, pool, widths, alone = stream_setup
     reqs = S.make_requests(pool, 40, widths, {"sf": 0.7, "bs": 0.3}, seed=6)
-    eng = S.ServingEngine(kinds, budget_bytes=9 << 20, max_batch_rows=2048, stage_bytes=8 << 20)
+    eng = S.ServingEngine(kinds, budget_bytes=18 << 20, max_batch_rows=2048, stage_bytes=8 << 20)
     st = eng.serve(reqs, None, keep_results=True)
     assert st["admission_waits"] > 0, st
     assert st["max_batch_requests"] > 1, st
