@@ -723,6 +723,7 @@ static int build_bs_impl(ld_descriptor *d, double rfac0, int J, int style, doubl
     ar.add(task2_v, &b.task2_v);
     ar.add(oslot, &b.oslot);
     ar.add(zg, &b.zg);
+    b.nzg = (int)zg.size();
     ar.add(zoff_f, &b.zoff_f);
     ar.add(zitem_f, &b.zitem_f);
     ar.add(ztoff_f, &b.ztoff_f);

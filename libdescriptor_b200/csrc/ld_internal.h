@@ -144,6 +144,7 @@ struct BSDev {
     // mb, mb) (zero outside the triple's range), q padded to even, at zg +
     // the triple's ztl y field
     const double *zg = nullptr;
+    int nzg = 0;
     const int *zoff_f = nullptr, *zitem_f = nullptr, *ztoff_f = nullptr;
     const int4 *ztl_f = nullptr;
     const int *zoff_v = nullptr, *zitem_v = nullptr, *ztoff_v = nullptr;
@@ -217,11 +218,15 @@ constexpr int kZWarps = LD_ZWARPS;
 // elements before and J/2+1 after (reads just outside a row land there or
 // in other elements of the lane, always finite, and meet a zero weight),
 // then the descriptor sums [lane][slot]
-inline size_t bs_smemZ_bytes(const BSDev &p) {
-    return (size_t)(p.J + 1 + p.nU + p.J / 2 + 1) * 32 * 16 + (size_t)32 * (p.nbslot > 0 ? p.nbslot : 1) * 8;
+inline size_t bs_smemZ_bytes(const BSDev &p, bool with_g = false) {
+    return (size_t)(p.J + 1 + p.nU + p.J / 2 + 1) * 32 * 16 + (size_t)32 * (p.nbslot > 0 ? p.nbslot : 1) * 8 +
+           (with_g ? (size_t)p.nzg * 8 + (size_t)p.ntrip * 32 * 8 : 0);
 }
-// the split form runs where its Z kernel fits one SM's shared memory
+// the split form runs where its Z kernel fits one SM's shared memory; the
+// column weights and the rows' betaj join the U block there when they fit
+// too
 inline bool bs_split(const BSDev &p) { return LD_BS_SPLIT != 0 && bs_smemZ_bytes(p) <= 227 * 1024; }
+inline bool bs_split_gshared(const BSDev &p) { return bs_smemZ_bytes(p, true) <= 227 * 1024; }
 
 // warps of the twojmax-specialised per-centre bispectrum CTA (4..8): enough
 // neighbour slots for about 32 neighbours in one round
