@@ -43,11 +43,14 @@ sys.path.insert(0, ROOT)
 METRIC = "desc+VJP atoms/s, 1 B200: served batch vs plain call; p50/p99 ms @≤1e-10 rel"
 from libdescriptor_b200.replicas import replica_throughput  # noqa: E402
 # DRAM bytes (read + write) per centre atom of the dominant kernels, from one
-# ncu capture each (profiles/): bispectrum 2J=8 pass (bsA + bsR, 8192-atom
-# launch: 5.03 MB + 21.98 MB) and the factored symmetry-function kernel
-# (4096-atom launch: 1.75 MB).  Traffic grows with the centres processed, so
-# other launch sizes are scaled by their atom counts.
-DRAM_BYTES_PER_ATOM = {"bs8": (5.027072e6 + 21.975296e6) / 8192, "sf24": 1.747968e6 / 4096}
+# ncu capture each (profiles/, cold caches): bispectrum 2J=8 pass (U kernel
+# bsA<8,0,1> 1.41 MB, Z kernel bsZ 41.50 MB -- of which the 37.4 MB U blocks
+# that the U kernel has just written, an L2 hit outside the profiler -- and
+# the pair gradient bsR 21.98 MB, 8192-atom launch) and the factored
+# symmetry-function kernel (4096-atom launch: 1.75 MB).  Traffic grows with
+# the centres processed, so other launch sizes are scaled by their atom counts.
+DRAM_BYTES_PER_ATOM = {"bs8": (1.414656e6 + 41.50528e6 + 21.975296e6) / 8192, "sf24": 1.747968e6 / 4096}
+BS_KERNELS = "bsA_kernel<8,0,1> (U) + bsZ_kernel<8,1,1> (Z, B, Y) + bsR_kernel<8> (pair gradient)"
 RATES = (1000.0, 10000.0, 50000.0)
 REQ_PER_STEP = 200
 MIX = {"sf": 0.7, "bs": 0.3}
@@ -385,7 +388,7 @@ def run_serve(args, torch, lds, dev, world, rank, local, dist):
             "traffic": DRAM_BYTES_PER_ATOM["bs8"] * bs_atoms_timed / K,
             "traffic_note": "bytes per step of the bispectrum lane, ncu DRAM bytes per atom of the 8192-atom "
                             "launch (profiles/) times the lane's atoms per step",
-            "kernel": "bsA_kernel<8,1> + bsR_kernel<8> (bispectrum 2J=8 lane of the batched pass)",
+            "kernel": BS_KERNELS + " (bispectrum 2J=8 lane of the batched pass)",
             "flops_per_step": bs_flops / K, "share_of_pass_time": ms.get("bs", 0.0) / tot_ms,
             "peak_source": "bench.py FP64 FMA probe (ld_measure_fp64_peak), same run; MEASURED_PEAKS.json has no "
                            "FP64 figure",
@@ -618,7 +621,7 @@ def run_single(args, torch, lds, dev, world, rank, local, dist):
     roof = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
             "traffic": DRAM_BYTES_PER_ATOM[args.workload] * n,
             "traffic_note": "ncu DRAM read + write bytes of one launch (profiles/)",
-            "kernel": "bsA_kernel<8,1> + bsR_kernel<8>" if spec["kind"] == "bs" else "sfg_kernel<1,1,0>",
+            "kernel": BS_KERNELS if spec["kind"] == "bs" else "sfg_kernel<1,1,0>",
             "flops_per_step": flop, "peak_source": "bench.py FP64 FMA probe (ld_measure_fp64_peak), same run",
             "call_weights_flops": {k: round(v, 1) for k, v in weights.items()},
             "hbm_bytes_per_step_algorithmic": int(cfg.coords.nbytes + cfg.nbl.nbytes + 8 * n * W * 2

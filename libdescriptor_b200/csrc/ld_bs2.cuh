@@ -13,9 +13,14 @@
 // mirrored.  NC = J/2+1 lanes serve one neighbour ("slot"); a warp holds
 // 32/NC slots.
 //
-// bsA_kernel<J, VJP>  one CTA per centre: stage neighbours, U (column lanes,
-//                     slots reduced through a per-warp buffer), Z (LPT task
-//                     lists), B; for the gradient also Y = sum betaj Z -> HBM.
+// bsA_kernel<J, VJP, UOUT>  one CTA per centre: stage neighbours, U (column
+//                     lanes, slots reduced through a per-warp buffer), Z (LPT
+//                     task lists), B; for the gradient also Y = sum betaj Z ->
+//                     HBM.  UOUT (the split form's first kernel): U only,
+//                     written as full U blocks [row / 32][element][row % 32].
+// bsZ_kernel<J, VJP, GSH>  split form: one CTA per 32 rows, a row per lane;
+//                     warp-uniform Z by rotating register windows over the
+//                     rows' U in shared memory, B, and Y = sum betaj Z -> HBM.
 // bsR_kernel<J>       pair-parallel gradient, reverse mode: one slot per
 //                     (centre, neighbour) pair runs the column recursion
 //                     forward (layer inputs kept in shared memory) and then
