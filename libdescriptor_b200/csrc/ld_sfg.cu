@@ -194,26 +194,36 @@ sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue)
 #if LD_SFG_GP_SHARED
             if (VJP) __syncwarp();
 #endif
-            int jj = 0, kk = 0;
-            {
-                int rem = lane;
-                while (jj < n - 1 && rem >= n - 1 - jj) {
-                    rem -= n - 1 - jj;
-                    ++jj;
-                }
-                kk = jj + 1 + rem;
-            }
-            while (jj < n - 1) {
-                if (S.inc[jj] && S.inc[kk]) {
-                    const int ks = S.spec[kk], js = S.spec[jj];
+            // Lane l owns neighbours jj = l, l + 32, ...; at step dd it takes the
+            // triplet (jj, kk = (jj + dd) mod n), dd = 1 .. n/2 (the last step,
+            // for even n, only for jj < n/2): every unordered pair once, and
+            // within a step the lanes' kk are distinct, so the kk gradients are
+            // plain read-modify-writes (steps ordered by __syncwarp) and the jj
+            // gradient stays in registers.
+            const int dmax = (n - 1) / 2, dlast = n / 2;
+            for (int m0 = 0; m0 < n; m0 += 32) {
+              const int jj = m0 + lane;
+              const bool own = jj < n;
+              const int jjs = own ? jj : 0;
+              const bool incj = own && S.inc[jjs];
+              const int js = S.spec[jjs];
+              const double cxj = S.cx[jjs], cyj = S.cy[jjs], czj = S.cz[jjs];
+              const double av = S.r[jjs], ia = S.ir[jjs], fa = S.fc[jjs];
+              const double dfa = VJP ? S.dfc[jjs] : 0.0;
+              double gjx = 0.0, gjy = 0.0, gjz = 0.0;
+              for (int dd = 1; dd <= dlast; ++dd) {
+                int kk = jj + dd;
+                if (kk >= n) kk -= n;
+                if (incj && (dd <= dmax || jj < dlast) && S.inc[kk]) {
+                    const int ks = S.spec[kk];
                     const double rcjk = p.rcut[js * p.ns + ks];
-                    const double jkx = S.cx[kk] - S.cx[jj], jky = S.cy[kk] - S.cy[jj], jkz = S.cz[kk] - S.cz[jj];
+                    const double jkx = S.cx[kk] - cxj, jky = S.cy[kk] - cyj, jkz = S.cz[kk] - czj;
                     const double d = sqrt(jkx * jkx + jky * jky + jkz * jkz);
-                    const double av = S.r[jj], b = S.r[kk];
-                    const double ia = S.ir[jj], ib = S.ir[kk];
+                    const double b = S.r[kk];
+                    const double ib = S.ir[kk];
                     const double asq = av * av, bsq = b * b, dsq = d * d;
                     const double cth = (asq + bsq - dsq) * (0.5 * ia * ib);
-                    const double fa = S.fc[jj], fb = S.fc[kk];
+                    const double fb = S.fc[kk];
                     double fd = 0.0, dfd = 0.0;
                     if (HAS4 && d < rcjk) {
                         const double t = kPi * d / rcjk;
@@ -314,7 +324,7 @@ sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue)
                     if (VJP) {
                         const double F4 = Fq[0], F5 = Fq[1];
                         const double A4 = Aq[0], B4 = Bq[0], C4 = Cq[0], A5 = Aq[1], B5 = Bq[1], C5 = Cq[1];
-                        const double dfa = S.dfc[jj], dfb = S.dfc[kk];
+                        const double dfb = S.dfc[kk];
                         const double dca = (asq - bsq + dsq) * (0.5 * ia * ia * ib);
                         const double dcb = (bsq - asq + dsq) * (0.5 * ia * ib * ib);
                         const double dcd = -d * ia * ib;
@@ -324,28 +334,29 @@ sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue)
                                           F5 * C5 * dcb - 2.0 * b * F5 * B5 + fa * dfb * A5;
                         const double Gd = F4 * C4 * dcd - 2.0 * d * F4 * B4 + fa * fb * dfd * A4 + F5 * C5 * dcd;
                         const double id = d > 0 ? 1.0 / d : 0.0;
-                        const double ijx = (S.cx[jj] - cix) * ia, ijy = (S.cy[jj] - ciy) * ia,
-                                     ijz = (S.cz[jj] - ciz) * ia;
+                        const double ijx = (cxj - cix) * ia, ijy = (cyj - ciy) * ia, ijz = (czj - ciz) * ia;
                         const double ukx = (S.cx[kk] - cix) * ib, uky = (S.cy[kk] - ciy) * ib,
                                      ukz = (S.cz[kk] - ciz) * ib;
                         const double udx = jkx * id, udy = jky * id, udz = jkz * id;
-                        atomicAdd(&S.gx[jj], Ga * ijx - Gd * udx);
-                        atomicAdd(&S.gy[jj], Ga * ijy - Gd * udy);
-                        atomicAdd(&S.gz[jj], Ga * ijz - Gd * udz);
-                        atomicAdd(&S.gx[kk], Gb * ukx + Gd * udx);
-                        atomicAdd(&S.gy[kk], Gb * uky + Gd * udy);
-                        atomicAdd(&S.gz[kk], Gb * ukz + Gd * udz);
+                        gjx += Ga * ijx - Gd * udx;
+                        gjy += Ga * ijy - Gd * udy;
+                        gjz += Ga * ijz - Gd * udz;
+                        S.gx[kk] += Gb * ukx + Gd * udx;
+                        S.gy[kk] += Gb * uky + Gd * udy;
+                        S.gz[kk] += Gb * ukz + Gd * udz;
                         gix -= Ga * ijx + Gb * ukx;
                         giy -= Ga * ijy + Gb * uky;
                         giz -= Ga * ijz + Gb * ukz;
                     }
                 }
-                int rem = kk - (jj + 1) + 32;
-                while (jj < n - 1 && rem >= n - 1 - jj) {
-                    rem -= n - 1 - jj;
-                    ++jj;
-                }
-                kk = jj + 1 + rem;
+                __syncwarp();
+              }
+              if (VJP && own) {
+                  S.gx[jj] += gjx;
+                  S.gy[jj] += gjy;
+                  S.gz[jj] += gjz;
+              }
+              __syncwarp();
             }
 #pragma unroll
             for (int ty = 0; ty < NT; ++ty)
