@@ -156,18 +156,20 @@ sf_kernel(SFDev p, RowArgs a, int per_warp_doubles, int *queue) {
             double acc3[M3];
 #pragma unroll
             for (int q = 0; q < M3; ++q) acc3[q] = 0.0;
-            int jj = 0, kk = 0;
-            {
-                int rem = lane;
-                while (jj < n - 1 && rem >= n - 1 - jj) {
-                    rem -= n - 1 - jj;
-                    ++jj;
-                }
-                kk = jj + 1 + rem;
-            }
+            // lane l owns neighbours jj = l, l + 32, ...; at step dd it takes the
+            // triplet (jj, kk = (jj + dd) mod n), dd = 1 .. n/2 (the last step,
+            // for even n, only for jj < n/2): every unordered pair once, the
+            // lanes' kk distinct within a step (plain read-modify-writes of the
+            // kk gradients, steps ordered by __syncwarp), jj's in registers
             __syncwarp();
-            while (jj < n - 1) {
-                if (S.inc[jj] && S.inc[kk]) {
+            const int dmax = (n - 1) / 2, dlast = n / 2;
+            for (int m0 = 0; m0 < n; m0 += 32) {
+              const int jj = m0 + lane;
+              double gjx = 0.0, gjy = 0.0, gjz = 0.0;
+              for (int dd = 1; dd <= dlast; ++dd) {
+                int kk = jj + dd;
+                if (kk >= n) kk -= n;
+                if (jj < n && (dd <= dmax || jj < dlast) && S.inc[jj] && S.inc[kk]) {
                     // r_ik and its cutoff functions are the staged pair values of kk
                     // (same coordinates, same species-pair cutoff as the reference's
                     // per-triplet recomputation)
@@ -283,24 +285,25 @@ sf_kernel(SFDev p, RowArgs a, int per_warp_doubles, int *queue) {
                         const double ukx = (S.cx[kk] - cix) * ib, uky = (S.cy[kk] - ciy) * ib,
                                      ukz = (S.cz[kk] - ciz) * ib;
                         const double udx = jkx * id, udy = jky * id, udz = jkz * id;
-                        atomicAdd(&S.gx[jj], Ga * ijx - Gd * udx);
-                        atomicAdd(&S.gy[jj], Ga * ijy - Gd * udy);
-                        atomicAdd(&S.gz[jj], Ga * ijz - Gd * udz);
-                        atomicAdd(&S.gx[kk], Gb * ukx + Gd * udx);
-                        atomicAdd(&S.gy[kk], Gb * uky + Gd * udy);
-                        atomicAdd(&S.gz[kk], Gb * ukz + Gd * udz);
+                        gjx += Ga * ijx - Gd * udx;
+                        gjy += Ga * ijy - Gd * udy;
+                        gjz += Ga * ijz - Gd * udz;
+                        S.gx[kk] += Gb * ukx + Gd * udx;
+                        S.gy[kk] += Gb * uky + Gd * udy;
+                        S.gz[kk] += Gb * ukz + Gd * udz;
                         gix -= Ga * ijx + Gb * ukx;
                         giy -= Ga * ijy + Gb * uky;
                         giz -= Ga * ijz + Gb * ukz;
                     }
                 }
-                // advance 32 triplets along the flattened upper triangle
-                int rem = kk - (jj + 1) + 32;
-                while (jj < n - 1 && rem >= n - 1 - jj) {
-                    rem -= n - 1 - jj;
-                    ++jj;
-                }
-                kk = jj + 1 + rem;
+                __syncwarp();
+              }
+              if (VJP && jj < n) {
+                  S.gx[jj] += gjx;
+                  S.gy[jj] += gjy;
+                  S.gz[jj] += gjz;
+              }
+              __syncwarp();
             }
 #pragma unroll
             for (int q = 0; q < M3; ++q) {
