@@ -31,6 +31,15 @@ constexpr int NA = kSFGA, NR = kSFGR;
 #endif
 constexpr int kGPExtra = (LD_SFG_GP_SHARED ? 2 * NA * NR : 0);
 
+// Paths the usual parameter sets never take (non-integer zeta, an eta that
+// is not an integer multiple of its group's smallest, cosine radial terms)
+// are kept out of line: with hundreds of rows per warp the warps of an SM
+// drift into different phases of the kernel, and the hot code must then fit
+// the instruction cache.
+__device__ __noinline__ double exp_cold(double x) { return exp(x); }
+__device__ __noinline__ double pow_cold(double b, double z) { return pow(b, z); }
+__device__ __noinline__ void sincos_cold(double x, double *s, double *c) { sincos(x, s, c); }
+
 template <bool VJP, bool HAS4, bool HAS5>
 __global__ void __launch_bounds__(kSFThreads, VJP ? LD_SFG_MINB : 4)
 sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue) {
@@ -136,7 +145,7 @@ sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue)
                             if (VJP) dv = e * (-2.0 * pa * (r - pb) * fc + dfc);
                         } else {
                             double sn, cs;
-                            sincos(pa * r, &sn, &cs);
+                            sincos_cold(pa * r, &sn, &cs);
                             v = cs * fc;
                             if (VJP) dv = -pa * sn * fc + cs * dfc;
                         }
@@ -255,7 +264,7 @@ sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue)
                             if (y < g.nr[ty]) {
                                 const int ec = g.ec[ty][y];
                                 if (y == 0 || ec < 2) {
-                                    E[y] = exp(-g.eta[ty][y] * Ssum);
+                                    E[y] = y == 0 ? exp(-g.eta[ty][y] * Ssum) : exp_cold(-g.eta[ty][y] * Ssum);
                                 } else {
                                     double rr = 1.0, xx = E[0];
                                     for (int k = ec; k > 0; k >>= 1) {
@@ -290,8 +299,8 @@ sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue)
                                         cp[x] = ipow(base, zi);
                                         dcp[x] = zi > 0 ? g.zeta[ty][x] * ipow(base, zi - 1) : 0.0;
                                     } else {
-                                        cp[x] = pow(base, g.zeta[ty][x]);
-                                        dcp[x] = g.zeta[ty][x] * pow(base, g.zeta[ty][x] - 1.0);
+                                        cp[x] = pow_cold(base, g.zeta[ty][x]);
+                                        dcp[x] = g.zeta[ty][x] * pow_cold(base, g.zeta[ty][x] - 1.0);
                                     }
                                 }
                             }
