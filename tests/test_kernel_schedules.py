@@ -1,0 +1,169 @@
+"""CPU: the index arithmetic that the GPU kernels' schedules rely on, restated
+loop for loop in Python and checked exhaustively over small sizes.
+
+* Symmetry-function triplet pairing (ld_sf.cu, ld_sfg.cu): lane l owns
+  neighbour jj = l (+32, ...) and at step dd takes (jj, (jj + dd) mod n),
+  dd = 1 .. n/2, the last step of an even n only for jj < n/2.  Every
+  unordered pair must come exactly once, and within one step the lanes'
+  second neighbours must be distinct (their gradients are then plain
+  read-modify-writes, no atomics).
+* Rows-in-lanes Z of the bispectrum (ld_bs2_impl.cuh, bsZ_kernel): the
+  window over u_{j1} with rotating registers, the per-triple column weights
+  G[mb][q] and the zero guards around the U block.  With arbitrary weights in
+  place of the Clebsch-Gordan table the model must equal the direct double
+  sum Z(ma, mb) = sum w(ma1, ma2) w(mb1, mb2) u1(ma1, mb1) u2(ma2, mb2), and
+  every read must stay inside guard + U + guard even when the guards and the
+  rest of the block hold non-zero values.
+* The U-only per-centre kernel's output (bsA_kernel UOUT): each left-half
+  element, its inversion image and the middle column's mirrored lower rows
+  must write every element of the full U exactly once, with the right
+  values.
+"""
+import numpy as np
+import pytest
+
+
+# ------------------------------------------------------- triplet pairing
+def _cyclic_steps(n):
+    """Per chunk of 32 lanes and step: list of (jj, kk) the lanes take."""
+    dmax, dlast = (n - 1) // 2, n // 2
+    steps = []
+    for m0 in range(0, n, 32):
+        for dd in range(1, dlast + 1):
+            pairs = []
+            for lane in range(32):
+                jj = m0 + lane
+                if jj >= n or not (dd <= dmax or jj < dlast):
+                    continue
+                pairs.append((jj, (jj + dd) % n))
+            steps.append(pairs)
+    return steps
+
+
+@pytest.mark.parametrize("n", list(range(0, 71)) + [96, 97, 128])
+def test_cyclic_pairing_covers_each_pair_once_with_distinct_kk(n):
+    seen = {}
+    for pairs in _cyclic_steps(n):
+        kks = [kk for _, kk in pairs]
+        assert len(kks) == len(set(kks)), (n, pairs)
+        for jj, kk in pairs:
+            assert jj != kk
+            key = (min(jj, kk), max(jj, kk))
+            seen[key] = seen.get(key, 0) + 1
+    assert len(seen) == n * (n - 1) // 2
+    assert all(v == 1 for v in seen.values())
+
+
+# ------------------------------------------------------ rows-in-lanes Z
+def _inversion_symmetric_u(J, rng):
+    U = []
+    for j in range(J + 1):
+        a = rng.normal(size=(j + 1, j + 1)) + 1j * rng.normal(size=(j + 1, j + 1))
+        for m in range(j + 1):
+            for k in range(j + 1):
+                if (m, k) < (j - m, j - k):
+                    a[j - m, j - k] = (-1) ** (m - k) * np.conj(a[m, k])
+                elif (m, k) == (j - m, j - k):
+                    a[m, k] = a[m, k].real if (m - k) % 2 == 0 else 1j * a[m, k].imag
+        U.append(a)
+    return U
+
+
+@pytest.mark.parametrize("J", [0, 1, 2, 5, 8])
+def test_rows_in_lanes_z_window_equals_direct_sum(J):
+    rng = np.random.default_rng(J)
+    U = _inversion_symmetric_u(J, rng)
+    ublock = [0]
+    for j in range(J + 1):
+        ublock.append(ublock[-1] + (j + 1) ** 2)
+    nU = ublock[-1]
+    glo, ghi = J + 1, J // 2 + 1
+    # guards and block filled with finite non-zero values: a read outside a
+    # row must meet a zero weight, not a zero value
+    mem = rng.normal(size=glo + nU + ghi) + 1j * rng.normal(size=glo + nU + ghi)
+    for j in range(J + 1):
+        mem[glo + ublock[j]:glo + ublock[j + 1]] = U[j].ravel()
+
+    def ld(e):
+        assert 0 <= glo + e < len(mem), ("read outside guard + U + guard", e)
+        return mem[glo + e]
+
+    trips = [(j1, j2, j) for j1 in range(J + 1) for j2 in range(j1 + 1)
+             for j in range(j1 - j2, min(J, j1 + j2) + 1, 2)]
+    for (j1, j2, j) in trips:
+        c, nc = (j1 + j2 - j) // 2, j // 2 + 1
+        w = rng.normal(size=(j1 + 1, j2 + 1))       # stands in for cg(j1, j2, j)
+        nst = min(j2, c + nc - 1) + 1
+        G = np.zeros((nst, nc))
+        for mb in range(nst):
+            for q in range(nc):
+                mb1 = c + q - mb
+                if 0 <= mb1 <= j1:
+                    G[mb, q] = w[mb1, mb]
+        for ma in range(j + 1):
+            z = np.zeros(nc, complex)
+            ca = c + ma
+            rem = nst % nc
+            for ma2 in range(max(0, ca - j1), min(j2, ca) + 1):
+                ma1 = ca - ma2
+                ga = w[ma1, ma2]
+                xrow = ublock[j2] + ma2 * (j2 + 1)
+                wrow = ublock[j1] + ma1 * (j1 + 1) + c - 1
+                win = [ga * ld(wrow + q + 1) for q in range(nc)]
+                for mb in range(rem):                      # shifting steps
+                    x = ld(xrow + mb)
+                    z += G[mb] * x * np.array(win)
+                    win = [ga * ld(wrow - mb)] + win[:-1]
+                for mb0 in range(rem, nst, nc):            # rotation blocks
+                    for s in range(nc):
+                        mb = mb0 + s
+                        x = ld(xrow + mb)
+                        for q in range(nc):
+                            z[q] += G[mb, q] * x * win[(q - s + nc) % nc]
+                        win[(nc - 1 - s) % nc] = ga * ld(wrow - mb)
+            for q in range(nc):
+                ref = 0j
+                for ma1 in range(j1 + 1):
+                    ma2 = ca - ma1
+                    if not 0 <= ma2 <= j2:
+                        continue
+                    for mb1 in range(j1 + 1):
+                        mb2 = c + q - mb1
+                        if 0 <= mb2 <= j2:
+                            ref += w[ma1, ma2] * w[mb1, mb2] * U[j1][ma1, mb1] * U[j2][ma2, mb2]
+                assert abs(z[q] - ref) <= 1e-12 * (1 + abs(ref)), (j1, j2, j, ma, q)
+
+
+# ------------------------------------------------- U-only output writer
+@pytest.mark.parametrize("J", list(range(0, 11)))
+def test_u_only_writer_fills_full_u_once(J):
+    rng = np.random.default_rng(100 + J)
+    U = _inversion_symmetric_u(J, rng)
+    wself = 1.0
+    ublock = [0]
+    for j in range(J + 1):
+        ublock.append(ublock[-1] + (j + 1) ** 2)
+    out = np.full(ublock[-1], np.nan, complex)
+    count = np.zeros(ublock[-1], int)
+    for jl in range(J + 1):
+        hj = jl // 2
+        for ma in range(jl + 1):
+            for m2 in range(hj + 1):                 # the left half, middle column whole
+                mir = jl % 2 == 0 and m2 == hj and ma > hj
+                if mir:                              # lower middle rows: mirror of row jl - ma
+                    v = U[jl][jl - ma, hj]
+                    sg = -1.0 if (ma - hj) & 1 else 1.0
+                    v = complex(sg * v.real, -sg * v.imag)
+                else:
+                    v = U[jl][ma, m2] + (wself if ma == m2 else 0.0)
+                k = ublock[jl] + ma * (jl + 1) + m2
+                out[k] = v
+                count[k] += 1
+                if jl - m2 > hj:                     # inversion image in the right half
+                    sg = -1.0 if (ma - m2) & 1 else 1.0
+                    k = ublock[jl] + (jl - ma) * (jl + 1) + (jl - m2)
+                    out[k] = complex(sg * v.real, -sg * v.imag)
+                    count[k] += 1
+    ref = np.concatenate([(U[j] + wself * np.eye(j + 1)).ravel() for j in range(J + 1)])
+    assert (count == 1).all()
+    np.testing.assert_allclose(out, ref, rtol=0, atol=1e-14)
