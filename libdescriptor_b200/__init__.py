@@ -12,7 +12,9 @@ files), ``compute`` / ``compute_batch`` / ``compute_single_atom``,
 of ``_lib/libldb200.so`` in FP64; there is no CPU fallback -- without a CUDA
 device the calls raise.
 
-Extras beyond the reference API: ``torch_ops`` (torch.autograd.Function over
+Extras beyond the reference API: ``gradient_params`` (dL/d(parameters) of a
+symmetry-function descriptor, which the reference computes with Enzyme and
+discards), ``torch_ops`` (torch.autograd.Function over
 device tensors), ``batch`` (one launch over many configurations, CUDA
 graphs, autotuning) and ``serving`` (continuous-batching request loop).
 """
@@ -49,6 +51,7 @@ gradient = _ext.gradient
 gradient_batch = _ext.gradient_batch
 gradient_single_atom = _ext.gradient_single_atom
 compute_and_gradient = _ext.compute_and_gradient
+gradient_params = _ext.gradient_params
 jacobian = _ext.jacobian
 num_gradient_single_atom = _ext.num_gradient_single_atom
 NeighList = _ext.NeighList
@@ -71,7 +74,7 @@ def measure_fp64_peak(iters: int = 4096) -> float:
 __all__ = [
     "AvailableDescriptors", "DescriptorKind", "compute", "compute_batch",
     "compute_single_atom", "gradient", "gradient_batch", "gradient_single_atom",
-    "compute_and_gradient",
+    "compute_and_gradient", "gradient_params",
     "jacobian", "num_gradient_single_atom", "NeighList", "create",
     "create_paddings", "launch_count", "measure_fp64_peak", "LIB_PATH",
 ]

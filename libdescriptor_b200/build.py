@@ -34,7 +34,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                      "-I" + INCLUDE, "-I" + CSRC] + os.environ.get("LDB_NVCC_DEFINES", "").split()
 CORE_SOURCES = ["ld_sf.cu", "ld_bs.cu", "ld_util.cu", "ld_core.cpp", "ld_neighbor.cpp", "ld_noalloc.cu",
                 "ld_bs2_j0_1_2_3_4.cu", "ld_bs2_j5_6.cu", "ld_bs2_j7.cu", "ld_bs2_j8.cu", "ld_bs2_j9.cu",
-                "ld_bs2_j10.cu", "ld_serve.cpp", "ld_sfg.cu", "ld_neighbor_dev.cu"]
+                "ld_bs2_j10.cu", "ld_serve.cpp", "ld_sfg.cu", "ld_neighbor_dev.cu", "ld_sfp.cu"]
 # host threads for the serving runtime's request staging
 EXTRA_FLAGS = {"ld_serve.cpp": ["-Xcompiler", "-fopenmp"]}
 HEADERS = [os.path.join(CSRC, "ld_internal.h"), os.path.join(CSRC, "ld_neighbor_math.h"), os.path.join(CSRC, "ld_sf_common.cuh"), os.path.join(CSRC, "ld_bs2.cuh"),

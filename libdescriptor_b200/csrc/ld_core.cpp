@@ -166,6 +166,8 @@ static int build_sf(ld_descriptor *d, int ns, const double *cutoff, int n_types,
     std::vector<double> a2, b2, P3, z3, l3, e3;
     struct Three { int o, t; double zeta, lam, eta; };
     std::vector<Three> three;
+    std::vector<int> pt, pofs;
+    std::vector<double> pv;
     int width = 0;
     size_t poff = 0;
     for (int b = 0; b < n_types; ++b) {
@@ -180,6 +182,9 @@ static int build_sf(ld_descriptor *d, int ns, const double *cutoff, int n_types,
         for (int q = 0; q < rows; ++q) {
             const double *pp = params ? params + poff + (size_t)q * cols : nullptr;
             const int o = width + q;
+            pt.push_back(t);
+            pofs.push_back((int)(poff + (size_t)q * cols));
+            for (int k = 0; k < 3; ++k) pv.push_back(k < need ? pp[k] : 0.0);
             if (t <= 3) {
                 o2.push_back(o);
                 t2.push_back(t);
@@ -309,6 +314,10 @@ static int build_sf(ld_descriptor *d, int ns, const double *cutoff, int n_types,
     ar.add(e3, &s.e3);
     ar.add(zi3, &s.zi3);
     ar.add(ec3, &s.ec3);
+    ar.add(pt, &s.pt);
+    ar.add(pofs, &s.pofs);
+    ar.add(pv, &s.pv);
+    s.nparams = (int)poff;
     int rc = ar.upload(d->tables);
     if (rc) return rc;
     d->kind = LD_KIND_SYMMETRY_FUNCTIONS;
@@ -1213,6 +1222,71 @@ int ld_gradient(ld_descriptor *d, int n_atoms, int n_total, const int *species, 
     if (rc) return rc;
     static const double dummy = 0.0;
     return host_pass(d, h, n_total, species, neighbor_list, coords, dE_ddesc ? dE_ddesc : &dummy, d_coords, desc_out);
+}
+
+static int gradient_params_impl(ld_descriptor *d, int n_atoms, int n_total, const int *species,
+                                const int *neighbor_list, const int *number_of_neighs, const double *coords,
+                                const double *dE_ddesc, double *d_params, int n_params) {
+    if (!d) return fail(LD_ERR_INVALID_ARG, "descriptor handle is NULL");
+    if (d->kind != LD_KIND_SYMMETRY_FUNCTIONS)
+        return fail(LD_ERR_INVALID_ARG, "parameter gradients are available for symmetry functions only");
+    if (n_params != d->sf.nparams)
+        return fail(LD_ERR_INVALID_ARG, "n_params=" + std::to_string(n_params) + " but the descriptor has " +
+                                            std::to_string(d->sf.nparams) + " parameters");
+    if (n_atoms < 0 || n_total < 0 || (n_atoms > 0 && (!number_of_neighs || !dE_ddesc || !species || !coords)))
+        return fail(LD_ERR_INVALID_ARG, "bad n_atoms / NULL input array");
+    if (n_params > 0 && !d_params) return fail(LD_ERR_INVALID_ARG, "d_params is NULL");
+    HostRows h;
+    int rc = make_rows(n_atoms, number_of_neighs, h);
+    if (rc) return rc;
+    if (h.nnz > 0 && !neighbor_list) return fail(LD_ERR_INVALID_ARG, "neighbor_list is NULL");
+    if ((rc = validate(d, h, n_total, species, neighbor_list))) return rc;
+    std::lock_guard<std::mutex> lk(d->mu);
+    if ((rc = ensure_stream(d)) || (rc = ensure_status(d))) return rc;
+    cudaStream_t s = d->stream;
+    const int W = d->width;
+    if ((rc = d->species.ensure(sizeof(int) * std::max(n_total, 1))) ||
+        (rc = d->nbl.ensure(sizeof(int) * std::max<long long>(h.nnz, 1))) ||
+        (rc = d->off.ensure(sizeof(long long) * (h.n_rows + 1))) ||
+        (rc = d->coords.ensure(sizeof(double) * 3 * std::max(n_total, 1))) ||
+        (rc = d->dE.ensure(sizeof(double) * std::max<size_t>((size_t)n_atoms * W, 1))) ||
+        (rc = d->dc.ensure(sizeof(double) * std::max(n_params, 1))))
+        return rc;
+    if (n_total) LDB_CUDA(cudaMemcpyAsync(d->species.p, species, sizeof(int) * n_total, cudaMemcpyHostToDevice, s));
+    if (h.nnz) LDB_CUDA(cudaMemcpyAsync(d->nbl.p, neighbor_list, sizeof(int) * h.nnz, cudaMemcpyHostToDevice, s));
+    LDB_CUDA(cudaMemcpyAsync(d->off.p, h.off.data(), sizeof(long long) * (h.n_rows + 1), cudaMemcpyHostToDevice, s));
+    if (n_total) LDB_CUDA(cudaMemcpyAsync(d->coords.p, coords, sizeof(double) * 3 * n_total, cudaMemcpyHostToDevice, s));
+    if (n_atoms) LDB_CUDA(cudaMemcpyAsync(d->dE.p, dE_ddesc, sizeof(double) * n_atoms * W, cudaMemcpyHostToDevice, s));
+    RowArgs a;
+    a.n_rows = n_atoms;
+    a.species = d->species.as<int>();
+    a.nbl = d->nbl.as<int>();
+    a.off = d->off.as<long long>();
+    a.max_neigh = std::max(h.maxn, 1);
+    a.coords = d->coords.as<double>();
+    a.n_total = n_total;
+    a.dE = d->dE.as<double>();
+    a.status = d->status.as<int>();
+    if ((rc = sf_param_launch(d->sf, a, d->dc.as<double>(), s))) return rc;
+    if (n_params) LDB_CUDA(cudaMemcpyAsync(d_params, d->dc.p, sizeof(double) * n_params, cudaMemcpyDeviceToHost, s));
+    return read_status(d, s);
+}
+
+int ld_gradient_params(ld_descriptor *d, int n_atoms, int n_total, const int *species, const int *neighbor_list,
+                       const int *number_of_neighs, const double *coords, const double *dE_ddesc, double *d_params,
+                       int n_params) {
+    try {
+        return gradient_params_impl(d, n_atoms, n_total, species, neighbor_list, number_of_neighs, coords, dE_ddesc,
+                                    d_params, n_params);
+    } catch (const std::bad_alloc &) {
+        return fail(LD_ERR_OOM, "host allocation failed");
+    }
+}
+
+int ld_num_params(const ld_descriptor *d, int *n_params) {
+    if (!d || !n_params) return fail(LD_ERR_INVALID_ARG, "ld_num_params: bad arguments");
+    *n_params = d->kind == LD_KIND_SYMMETRY_FUNCTIONS ? d->sf.nparams : 0;
+    return LD_OK;
 }
 
 int ld_compute_batch(ld_descriptor *d, int n_configs, const int *n_atoms, const int *config_ptr, int n_total,

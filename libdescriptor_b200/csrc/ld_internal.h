@@ -89,6 +89,14 @@ struct SFDev {
     const int *ec3 = nullptr;
     bool has_grid = false;
     SFGrid grid;
+    // hyperparameter gradients: per output its type code (1..5), the offset
+    // of its first parameter in the caller's flat parameter vector, and its
+    // parameters (g2: eta, Rs; g3: kappa; g4/g5: zeta, lambda, eta) at
+    // pv[3 * output]
+    int nparams = 0;
+    const int *pt = nullptr;
+    const int *pofs = nullptr;
+    const double *pv = nullptr;
 };
 
 // ------------------------------------------------------------- bispectrum
@@ -241,6 +249,7 @@ constexpr int bs2_warps(int J) {
 }
 
 int sf_launch(const SFDev &p, const RowArgs &a, cudaStream_t s);
+int sf_param_launch(const SFDev &p, const RowArgs &a, double *d_params, cudaStream_t s);
 int sfg_launch(const SFDev &p, const RowArgs &a, cudaStream_t s);
 int bs_launch(const BSDev &p, const RowArgs &a, cudaStream_t s);
 size_t sf_work_bytes(const SFDev &p, int n_rows, bool vjp);

@@ -240,6 +240,20 @@ PYBIND11_MODULE(_libdescriptor, m) {
         return out;
     });
 
+    // dL/d(parameters) of a symmetry-function descriptor, in the flat layout
+    // of the parameters given at init
+    m.def("gradient_params", [](Kind &ds, int n_atoms, IArr species, IArr neighbors, IArr number_of_neighbors,
+                                DArr coords, DArr dE_ddesc) {
+        if ((long long)dE_ddesc.size() < (long long)n_atoms * ds.width())
+            throw py::value_error("dE_ddesc must hold n_atoms * width values");
+        int np = 0;
+        check(ld_num_params(ds.get(), &np));
+        py::array_t<double> out(std::max(np, 0));
+        check(ld_gradient_params(ds.get(), n_atoms, (int)(coords.size() / 3), species.data(), neighbors.data(),
+                                 number_of_neighbors.data(), coords.data(), dE_ddesc.data(), out.mutable_data(), np));
+        return out;
+    });
+
     // desc + VJP in one fused pass (host buffers): returns (desc, gradient)
     m.def("compute_and_gradient", [](Kind &ds, int n_atoms, IArr species, IArr neighbors, IArr number_of_neighbors,
                                      DArr coords, DArr dE_ddesc) {
