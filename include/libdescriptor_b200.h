@@ -104,18 +104,19 @@ int ld_gradient(ld_descriptor *d, int n_atoms, int n_total, const int *species,
 /* Gradient of a loss with respect to the descriptor's parameters, the part
  * of the reference's Enzyme gradient that it computes into a shadow
  * DescriptorKind and then discards (src/Descriptors.cpp:165-215):
- * d_params[k] = sum_{i,o} dE_ddesc[i,o] d desc[i,o] / d params[k], in the
- * layout of the flat parameter vector given at init (g2 rows (eta, Rs), g3
- * (kappa), g4/g5 (zeta, lambda, eta); extra columns of a row get 0).
- * Symmetry functions only (LD_ERR_INVALID_ARG for the bispectrum);
+ * d_params[k] = sum_{i,o} dE_ddesc[i,o] d desc[i,o] / d params[k].
+ * Symmetry functions: in the layout of the flat parameter vector given at
+ * init (g2 rows (eta, Rs), g3 (kappa), g4/g5 (zeta, lambda, eta); extra
+ * columns of a row get 0).  Bispectrum: one value, dL/d rfac0.
  * n_params must equal ld_num_params. */
 int ld_gradient_params(ld_descriptor *d, int n_atoms, int n_total, const int *species,
                        const int *neighbor_list, const int *number_of_neighs,
                        const double *coords, const double *dE_ddesc, double *d_params,
                        int n_params);
 
-/* Length of the flat parameter vector of a symmetry-function descriptor
- * (0 for the bispectrum). */
+/* Number of values ld_gradient_params returns: the length of the flat
+ * parameter vector of a symmetry-function descriptor, 1 (rfac0) for the
+ * bispectrum. */
 int ld_num_params(const ld_descriptor *d, int *n_params);
 
 /* Descriptor::compute_batch (src/Descriptors.cpp:138-163). */

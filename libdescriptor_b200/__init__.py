@@ -12,9 +12,10 @@ files), ``compute`` / ``compute_batch`` / ``compute_single_atom``,
 of ``_lib/libldb200.so`` in FP64; there is no CPU fallback -- without a CUDA
 device the calls raise.
 
-Extras beyond the reference API: ``gradient_params`` (dL/d(parameters) of a
-symmetry-function descriptor, which the reference computes with Enzyme and
-discards), ``torch_ops`` (torch.autograd.Function over
+Extras beyond the reference API: ``gradient_params`` (dL/d(parameters):
+the symmetry functions' eta, Rs, kappa, zeta, lambda or the bispectrum's
+rfac0, which the reference computes with Enzyme and discards), ``torch_ops``
+(torch.autograd.Function over
 device tensors), ``batch`` (one launch over many configurations, CUDA
 graphs, autotuning) and ``serving`` (continuous-batching request loop).
 """

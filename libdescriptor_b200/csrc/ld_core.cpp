@@ -1228,11 +1228,13 @@ static int gradient_params_impl(ld_descriptor *d, int n_atoms, int n_total, cons
                                 const int *neighbor_list, const int *number_of_neighs, const double *coords,
                                 const double *dE_ddesc, double *d_params, int n_params) {
     if (!d) return fail(LD_ERR_INVALID_ARG, "descriptor handle is NULL");
-    if (d->kind != LD_KIND_SYMMETRY_FUNCTIONS)
-        return fail(LD_ERR_INVALID_ARG, "parameter gradients are available for symmetry functions only");
-    if (n_params != d->sf.nparams)
+    const bool bs = d->kind == LD_KIND_BISPECTRUM;
+    const int np_have = bs ? 1 : d->sf.nparams;
+    if (n_params != np_have)
         return fail(LD_ERR_INVALID_ARG, "n_params=" + std::to_string(n_params) + " but the descriptor has " +
-                                            std::to_string(d->sf.nparams) + " parameters");
+                                            std::to_string(np_have) + " parameters");
+    if (bs && d->bs.J > kMaxTwoJ)
+        return fail(LD_ERR_CAPACITY, "the rfac0 gradient needs twojmax <= " + std::to_string(kMaxTwoJ));
     if (n_atoms < 0 || n_total < 0 || (n_atoms > 0 && (!number_of_neighs || !dE_ddesc || !species || !coords)))
         return fail(LD_ERR_INVALID_ARG, "bad n_atoms / NULL input array");
     if (n_params > 0 && !d_params) return fail(LD_ERR_INVALID_ARG, "d_params is NULL");
@@ -1250,7 +1252,7 @@ static int gradient_params_impl(ld_descriptor *d, int n_atoms, int n_total, cons
         (rc = d->off.ensure(sizeof(long long) * (h.n_rows + 1))) ||
         (rc = d->coords.ensure(sizeof(double) * 3 * std::max(n_total, 1))) ||
         (rc = d->dE.ensure(sizeof(double) * std::max<size_t>((size_t)n_atoms * W, 1))) ||
-        (rc = d->dc.ensure(sizeof(double) * std::max(n_params, 1))))
+        (rc = d->dc.ensure(sizeof(double) * (std::max(n_params, 1) + (bs ? 3 * (size_t)std::max(n_total, 1) : 0)))))
         return rc;
     if (n_total) LDB_CUDA(cudaMemcpyAsync(d->species.p, species, sizeof(int) * n_total, cudaMemcpyHostToDevice, s));
     if (h.nnz) LDB_CUDA(cudaMemcpyAsync(d->nbl.p, neighbor_list, sizeof(int) * h.nnz, cudaMemcpyHostToDevice, s));
@@ -1267,7 +1269,24 @@ static int gradient_params_impl(ld_descriptor *d, int n_atoms, int n_total, cons
     a.n_total = n_total;
     a.dE = d->dE.as<double>();
     a.status = d->status.as<int>();
-    if ((rc = sf_param_launch(d->sf, a, d->dc.as<double>(), s))) return rc;
+    if (bs) {
+        // the regular desc + VJP pass (coordinate gradient into scratch) with
+        // the pair kernel also summing dL/d rfac0
+        double *dp = d->dc.as<double>();
+        LDB_CUDA(cudaMemsetAsync(dp, 0, sizeof(double) * (1 + 3 * (size_t)std::max(n_total, 1)), s));
+        a.dcoords = dp + 1;
+        a.d_rfac0 = dp;
+        if (n_atoms > 0) {
+            size_t wb = 0;
+            if ((rc = ld_rows_work_bytes(d, n_atoms, 1, &wb))) return rc;
+            if ((rc = d->work.ensure(wb))) return rc;
+            a.work = d->work.p;
+            a.work_bytes = wb;
+            if ((rc = launch_rows(d, a, s))) return rc;
+        }
+    } else if ((rc = sf_param_launch(d->sf, a, d->dc.as<double>(), s))) {
+        return rc;
+    }
     if (n_params) LDB_CUDA(cudaMemcpyAsync(d_params, d->dc.p, sizeof(double) * n_params, cudaMemcpyDeviceToHost, s));
     return read_status(d, s);
 }
@@ -1285,7 +1304,7 @@ int ld_gradient_params(ld_descriptor *d, int n_atoms, int n_total, const int *sp
 
 int ld_num_params(const ld_descriptor *d, int *n_params) {
     if (!d || !n_params) return fail(LD_ERR_INVALID_ARG, "ld_num_params: bad arguments");
-    *n_params = d->kind == LD_KIND_SYMMETRY_FUNCTIONS ? d->sf.nparams : 0;
+    *n_params = d->kind == LD_KIND_SYMMETRY_FUNCTIONS ? d->sf.nparams : 1;
     return LD_OK;
 }
 

@@ -177,6 +177,7 @@ struct RowArgs {
     double *desc = nullptr;            // nullable for gradient
     const double *dE = nullptr;        // nullptr = forward only
     double *dcoords = nullptr;
+    double *d_rfac0 = nullptr;         // bispectrum: dL/d rfac0 added here when set (pair kernel)
     long long dc_stride = 0;           // doubles between rows' gradients (0 = shared)
     const int *image = nullptr;
     int *status = nullptr;             // device error word

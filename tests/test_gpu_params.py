@@ -1,6 +1,7 @@
-"""GPU: gradients of a symmetry-function loss with respect to the descriptor's
-own parameters (eta, Rs, kappa, zeta, lambda) -- the part of the reference's
-Enzyme gradient that it computes into a shadow DescriptorKind and discards.
+"""GPU: gradients of a loss with respect to the descriptor's own parameters
+(symmetry functions: eta, Rs, kappa, zeta, lambda; bispectrum: rfac0) -- the
+part of the reference's Enzyme gradient that it computes into a shadow
+DescriptorKind and discards.
 
 Checked against central finite differences of the oracle's forward
 (the reference's forward restated in C) in every parameter:
@@ -74,14 +75,34 @@ def test_parameter_gradient_matches_oracle_fd(oracle_mod, kind):
     np.testing.assert_allclose(again, got, rtol=1e-12, atol=1e-12 * scale)
 
 
-def test_parameter_gradient_is_symmetry_functions_only():
+@pytest.mark.parametrize("twojmax", [6, 8])
+def test_rfac0_gradient_matches_oracle_fd(oracle_mod, twojmax):
+    """Bispectrum: the one parameter, rfac0 (it enters through theta0 of the
+    Cayley-Klein map); two species with different weights, switching on."""
     import libdescriptor_b200 as lds
     from libdescriptor_b200 import workloads as W
+    from oracle import OracleDescriptor
 
-    x, cell = W.diamond_cell(1, 1, 1, jitter=0.05, seed=1)
-    cfg = W.prepare(x, cell, np.zeros(len(x), np.int32), 5.0)
-    k = lds.DescriptorKind.init_descriptor(lds.AvailableDescriptors.Bispectrum, 0.99363, 6, 3, 0, 0.0, 1, 0, 5.0,
-                                           ["Si"], [1.0])
-    dE = np.zeros((cfg.n_atoms, int(k.width)))
-    with pytest.raises(ValueError):
-        lds.gradient_params(k, cfg.n_atoms, cfg.species, cfg.nbl, cfg.counts, cfg.coords, dE)
+    x, cell, sp = W.random_packing(48, density=0.05, dmin=2.0, n_species=2, seed=12)
+    cfg = W.prepare(x, cell, sp, 5.0)
+    rfac0, wts = 0.99363, [1.0, 0.5]
+    k = lds.DescriptorKind.init_descriptor(lds.AvailableDescriptors.Bispectrum, rfac0, twojmax, 3, 0, 0.0, 1, 0,
+                                           5.0, ["A", "B"], wts)
+    n = cfg.n_atoms
+    dE = np.random.default_rng(13).normal(size=(n, int(k.width)))
+    got = lds.gradient_params(k, n, cfg.species, cfg.nbl, cfg.counts, cfg.coords, dE)
+    assert got.shape == (1,)
+    cm = np.full((2, 2), 5.0)
+
+    def loss(rf):
+        o = OracleDescriptor.bispectrum(rf, twojmax, 3, 0.0, 1, 0, 2, cm, wts)
+        return float(np.sum(dE * o.run(n, cfg.species, cfg.nbl, cfg.counts, cfg.coords)))
+
+    h = 1e-6 * rfac0
+    fd = (loss(rfac0 + h) - loss(rfac0 - h)) / (2 * h)
+    assert abs(got[0] - fd) <= FD_RTOL * abs(fd), (got[0], fd)
+    # the coordinate gradient of the same pass is unaffected
+    desc0 = np.zeros((n, int(k.width)))
+    ref = lds.gradient(k, n, cfg.species, cfg.nbl, cfg.counts, cfg.coords, desc0, dE)
+    again = lds.gradient(k, n, cfg.species, cfg.nbl, cfg.counts, cfg.coords, desc0, dE)
+    np.testing.assert_allclose(again, ref, rtol=1e-12, atol=1e-12 * np.max(np.abs(ref)))
