@@ -260,5 +260,10 @@ size_t bs_smem_bytes(const BSDev &p, int max_neigh, bool vjp);
 int offsets_launch(int n_rows, const int *counts, long long *off, int *maxn,
                    void *tmp, size_t tmp_bytes, cudaStream_t s);
 size_t offsets_tmp_bytes(int n_rows);
+// Stream-ordered scratch (free it with cudaFreeAsync) from a memory pool the
+// library owns on each device.  The pool keeps what is freed (no release
+// threshold), so calls that need scratch again reuse it instead of going back
+// to the driver; it holds up to the largest scratch any call has needed.
+int pool_alloc(void **p, size_t bytes, cudaStream_t s);
 
 }  // namespace ldb

@@ -229,8 +229,8 @@ struct Scratch {
     template <class T>
     int get(T **p, size_t count) {
         void *q = nullptr;
-        cudaError_t e = cudaMallocAsync(&q, (count ? count : 1) * sizeof(T), s);
-        if (e != cudaSuccess) return cuda_fail(e, "neighbour builder scratch");
+        const int rc = pool_alloc(&q, (count ? count : 1) * sizeof(T), s);
+        if (rc) return rc;
         ptrs.push_back(q);
         *p = static_cast<T *>(q);
         return LD_OK;

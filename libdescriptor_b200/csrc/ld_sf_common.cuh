@@ -100,7 +100,8 @@ int launch_rows_kernel(K kern, const P &p, const RowArgs &a, cudaStream_t s, boo
             if (a.work_bytes < sizeof(int)) return fail(LD_ERR_INVALID_ARG, "work space too small");
             queue = static_cast<int *>(a.work);
         } else {
-            LDB_CUDA(cudaMallocAsync((void **)&queue, sizeof(int), s));
+            const int rc = pool_alloc((void **)&queue, sizeof(int), s);
+            if (rc) return rc;
             own = true;
         }
         LDB_CUDA(cudaMemsetAsync(queue, 0, sizeof(int), s));

@@ -1,5 +1,6 @@
 // ld_util.cu -- small device utilities: CSR row offsets, the FP64 rate probe.
 #include <cub/cub.cuh>
+#include <mutex>
 
 #include "ld_internal.h"
 
@@ -60,6 +61,38 @@ __global__ void op_probe(int op, int iters, double *out) {
 }
 
 }  // namespace
+
+int pool_alloc(void **p, size_t bytes, cudaStream_t s) {
+    constexpr int kMaxDevices = 64;
+    static std::mutex mu;
+    static cudaMemPool_t pools[kMaxDevices] = {};
+    int dev = 0;
+    LDB_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return fail(LD_ERR_INVALID_ARG, "device ordinal outside the pool table");
+    cudaMemPool_t pool = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (!pools[dev]) {
+            cudaMemPoolProps props = {};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.handleTypes = cudaMemHandleTypeNone;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            cudaMemPool_t created = nullptr;
+            LDB_CUDA(cudaMemPoolCreate(&created, &props));
+            unsigned long long keep = ~0ull;
+            cudaError_t e = cudaMemPoolSetAttribute(created, cudaMemPoolAttrReleaseThreshold, &keep);
+            if (e != cudaSuccess) {
+                cudaMemPoolDestroy(created);
+                return cuda_fail(e, "scratch pool");
+            }
+            pools[dev] = created;
+        }
+        pool = pools[dev];
+    }
+    LDB_CUDA(cudaMallocFromPoolAsync(p, bytes ? bytes : 1, pool, s));
+    return LD_OK;
+}
 
 size_t offsets_tmp_bytes(int n_rows) {
     size_t a = 0, b = 0;
