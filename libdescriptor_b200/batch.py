@@ -71,6 +71,10 @@ class DeviceBatch:
         dev = torch.device(device or "cuda")
 
         def t(a, dt):
+            # torch tensors (e.g. pinned host buffers) are copied without
+            # blocking the host, numpy arrays through a pageable copy
+            if isinstance(a, torch.Tensor):
+                return a.to(device=dev, dtype=dt, non_blocking=True)
             return torch.from_numpy(np.ascontiguousarray(a)).to(device=dev, dtype=dt)
 
         n_rows = int(b.n_rows)
@@ -79,10 +83,10 @@ class DeviceBatch:
         s = stream if stream is not None else torch.cuda.current_stream(dev)
         mx = int(_ext._neighbor_offsets_dev(kind, n_rows, counts.data_ptr(), off.data_ptr(), True, s.cuda_stream))
         row_ptr = np.concatenate([[0], np.cumsum(b.n_atoms)]).astype(np.int64)
+        nbl = b.nbl if (b.nbl.numel() if isinstance(b.nbl, torch.Tensor) else b.nbl.size) else np.zeros(1, np.int32)
         return cls(n_rows, int(b.coords.shape[0]), np.asarray(b.n_atoms), row_ptr, np.asarray(b.config_ptr),
                    t(b.coords, torch.float64), t(b.species, torch.int32), t(b.image, torch.int32),
-                   t(b.nbl if b.nbl.size else np.zeros(1, np.int32), torch.int32), counts, off,
-                   t(b.row_centre, torch.int32), max(mx, 1))
+                   t(nbl, torch.int32), counts, off, t(b.row_centre, torch.int32), max(mx, 1))
 
     @property
     def n_configs(self) -> int:
