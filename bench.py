@@ -643,19 +643,25 @@ def run_single(args, torch, lds, dev, world, rank, local, dist):
     tot_ms = float(sum(a.elapsed_time(b) for a, b in evs))
     value, tot_ms, _ = replica_throughput(n * args.steps, tot_ms, dist, dev)
     ms_per_step = tot_ms / args.steps
+    # the call a user makes, with its inputs staged in pinned host memory
+    def pinned(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+
+    h_sp, h_nbl, h_cnt, h_x, h_dE = (pinned(cfg.species), pinned(cfg.nbl), pinned(cfg.counts), pinned(cfg.coords),
+                                     pinned(dE_h))
     for _ in range(2):
-        lds.compute_and_gradient(ds, n, cfg.species, cfg.nbl, cfg.counts, cfg.coords, dE_h)
+        lds.compute_and_gradient(ds, n, h_sp, h_nbl, h_cnt, h_x, h_dE)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     ke = max(3, min(args.steps, 10))
     for _ in range(ke):
-        lds.compute_and_gradient(ds, n, cfg.species, cfg.nbl, cfg.counts, cfg.coords, dE_h)
+        lds.compute_and_gradient(ds, n, h_sp, h_nbl, h_cnt, h_x, h_dE)
     e2e_s = (time.perf_counter() - t0) / ke
     h2d = cfg.species.nbytes + cfg.nbl.nbytes + cfg.counts.nbytes + cfg.coords.nbytes + dE_h.nbytes + 8 * (n + 1)
     d2h = 8 * n * W + 8 * 3 * cfg.n_total
     e2e = {"value": world * n / e2e_s, "unit": "atoms/s", "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * e2e_s,
-           "api": "libdescriptor_b200.compute_and_gradient (host numpy in/out, one fused pass)"}
+           "api": "libdescriptor_b200.compute_and_gradient (numpy inputs in pinned host memory, numpy results out, one fused pass)"}
     if rank != 0:
         return None
     flop = algorithmic_flops(spec, cfg, weights)
