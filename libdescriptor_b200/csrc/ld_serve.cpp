@@ -11,6 +11,7 @@
 #include <cstdint>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 #include <algorithm>
 
@@ -123,7 +124,9 @@ extern "C" int ld_stage_request(int n_atoms, int n_total, long long nnz, int wid
     }
     int bad = 0;
     const int np = (int)pieces.size();
-    const int nthr = (int)std::max(1LL, std::min<long long>(8, total / (4 * kChunkBytes)));
+    // one host thread per MiB of copying, up to the cores (at most 16)
+    static const int kCores = std::max(1, std::min(16, (int)std::thread::hardware_concurrency()));
+    const int nthr = (int)std::max(1LL, std::min<long long>(kCores, total / kChunkBytes));
 #pragma omp parallel for num_threads(nthr) schedule(dynamic, 1) reduction(| : bad) if (nthr > 1)
     for (int i = 0; i < np; ++i) {
         const Piece &pc = pieces[i];
