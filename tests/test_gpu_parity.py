@@ -34,6 +34,26 @@ def test_gradient_matches_oracle(oracle_mod, name):
     assert_close(desc, g["desc"], DESC_RTOL, name + " desc of the fused pass")
 
 
+@pytest.mark.parametrize("name", [n for n in golden_names() if n.startswith("sf")])
+def test_table_driven_sf_kernel_matches(oracle_mod, name):
+    """The table-driven symmetry-function kernel (any parameter set; chosen
+    when a set does not factor into a (lambda, zeta) x eta grid), forced on
+    the symmetry-function goldens: forward vs the reference, fused VJP vs the
+    oracle."""
+    g = load_golden(name)
+    h = gpu_for(name, g)
+    h.set_tuning(4, 1)
+    o = oracle_for(name, g)
+    n = int(g["n_atoms"])
+    desc = h.compute(n, g["species"], g["nbl"], g["counts"], g["coords"])
+    assert_close(desc, g["desc"], DESC_RTOL, name + " table-driven desc")
+    dE = np.random.default_rng(4).normal(size=(n, h.width))
+    dc, desc2 = h.gradient(n, g["species"], g["nbl"], g["counts"], g["coords"], dE, want_desc=True)
+    _, dco = o.run(n, g["species"], g["nbl"], g["counts"], g["coords"], dE=dE)
+    assert_close(dc, dco, GRAD_RTOL, name + " table-driven grad")
+    assert_close(desc2, g["desc"], DESC_RTOL, name + " table-driven desc of the fused pass")
+
+
 @pytest.mark.parametrize("name", [n for n in golden_names() if load_golden(n).get("fd_index") is not None
                                   and len(load_golden(n)["fd_index"])])
 def test_gradient_matches_reference_fd(name):
