@@ -40,7 +40,9 @@ __device__ __noinline__ double exp_cold(double x) { return exp(x); }
 __device__ __noinline__ double pow_cold(double b, double z) { return pow(b, z); }
 __device__ __noinline__ void sincos_cold(double x, double *s, double *c) { sincos(x, s, c); }
 
-template <bool VJP, bool HAS4, bool HAS5>
+// PH: 0 both sums, 2 the two-body sums only, 3 the three-body sums only
+// (large batches run 2 then 3, see launch_g)
+template <bool VJP, bool HAS4, bool HAS5, int PH = 0>
 __global__ void __launch_bounds__(kSFThreads, VJP ? LD_SFG_MINB : 4)
 sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue) {
     extern __shared__ double smem[];
@@ -116,7 +118,7 @@ sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue)
         const double *dE = VJP ? a.dE + (size_t)cur_row * width : nullptr;
         double gix = 0.0, giy = 0.0, giz = 0.0;
         // ---- two-body terms
-        if (g.n2 > 0) {
+        if (PH != 3 && g.n2 > 0) {
             double acc2[kSFG2];
 #pragma unroll
             for (int q = 0; q < kSFG2; ++q) acc2[q] = 0.0;
@@ -175,7 +177,7 @@ sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue)
             }
         }
         // ---- three-body terms
-        if (HAS4 || HAS5) {
+        if (PH != 2 && (HAS4 || HAS5)) {
             constexpr int NT = 2;
             double acc[NT][NA][NR];
 #if LD_SFG_GP_SHARED
@@ -403,8 +405,21 @@ sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue)
     }
 }
 
+// Batches of at least this many rows run the two-body and the three-body
+// sums as two launches: with hundreds of rows per warp the warps of an SM
+// drift into different phases of the kernel, and a launch that holds one
+// phase keeps its hot code in the instruction cache (the rows' neighbours
+// are staged twice; 0 disables the split)
+#ifndef LD_SFG_SPLIT_ROWS
+#define LD_SFG_SPLIT_ROWS 32768
+#endif
 template <bool VJP, bool H4, bool H5>
 int launch_g(const SFDev &p, const RowArgs &a, cudaStream_t s) {
+    if (LD_SFG_SPLIT_ROWS > 0 && a.n_rows >= LD_SFG_SPLIT_ROWS && p.grid.n2 > 0 && (H4 || H5)) {
+        int rc = launch_rows_kernel(sfg_kernel<VJP, H4, H5, 2>, p, a, s, VJP, "sfg_kernel", VJP ? kGPExtra : 0);
+        if (rc) return rc;
+        return launch_rows_kernel(sfg_kernel<VJP, H4, H5, 3>, p, a, s, VJP, "sfg_kernel", VJP ? kGPExtra : 0);
+    }
     return launch_rows_kernel(sfg_kernel<VJP, H4, H5>, p, a, s, VJP, "sfg_kernel", VJP ? kGPExtra : 0);
 }
 

@@ -230,3 +230,34 @@ def test_torch_autograd_function(kind):
             lm = float((T.descriptors(k, xm, rows) * wt).sum())
             fd = (lp - lm) / (2 * hstep)
             assert abs(fd - g[a, d]) <= 1e-6 * max(1.0, abs(g[a, d])), (a, d, fd, g[a, d])
+
+
+def test_large_sf_batch_split_launches_match_per_config():
+    """A symmetry-function batch of at least 32768 rows runs its two-body and
+    three-body sums as two launches; each of its 4096-atom cells alone runs
+    the single kernel.  Both give the same descriptors and forces."""
+    import libdescriptor_b200 as lds
+    from libdescriptor_b200 import batch as B
+    from libdescriptor_b200 import workloads as W
+
+    cfgs = []
+    for c in range(8):
+        x, cell = W.diamond_cell(8, 8, 8, jitter=0.1, strain=0.02, seed=200 + c)
+        cfgs.append(W.prepare(x, cell, np.zeros(len(x), np.int32), 5.0))
+    b = W.concat(cfgs)
+    assert b.n_rows >= 32768
+    k = _module_kind("sf")
+    dE = np.random.default_rng(31).normal(size=(b.n_rows, int(k.width)))
+    db = B.DeviceBatch.from_batch(b, k)
+    ps = B.BatchedPass(k, db, _dev(dE, torch.float64))
+    ps.run()
+    ps.sync_status()
+    desc, grad = ps.desc.cpu().numpy(), ps.grad.cpu().numpy()
+    r0 = 0
+    for c, cfg in enumerate(cfgs):
+        n = cfg.n_atoms
+        d1, g1 = lds.compute_and_gradient(k, n, cfg.species, cfg.nbl, cfg.counts, cfg.coords, dE[r0:r0 + n])
+        p = int(b.config_ptr[c])
+        assert_close(desc[r0:r0 + n], d1, DESC_RTOL, f"cell {c} desc")
+        assert_close(grad[p:p + n], W.fold(g1, n, cfg.image), GRAD_RTOL, f"cell {c} forces")
+        r0 += n
