@@ -411,7 +411,7 @@ sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue)
 // phase keeps its hot code in the instruction cache (the rows' neighbours
 // are staged twice; 0 disables the split)
 #ifndef LD_SFG_SPLIT_ROWS
-#define LD_SFG_SPLIT_ROWS 32768
+#define LD_SFG_SPLIT_ROWS 8192
 #endif
 template <bool VJP, bool H4, bool H5>
 int launch_g(const SFDev &p, const RowArgs &a, cudaStream_t s) {

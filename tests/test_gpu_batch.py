@@ -233,7 +233,7 @@ def test_torch_autograd_function(kind):
 
 
 def test_large_sf_batch_split_launches_match_per_config():
-    """A symmetry-function batch of at least 32768 rows runs its two-body and
+    """A symmetry-function batch of at least 8192 rows runs its two-body and
     three-body sums as two launches; each of its 4096-atom cells alone runs
     the single kernel.  Both give the same descriptors and forces."""
     import libdescriptor_b200 as lds
@@ -245,7 +245,7 @@ def test_large_sf_batch_split_launches_match_per_config():
         x, cell = W.diamond_cell(8, 8, 8, jitter=0.1, strain=0.02, seed=200 + c)
         cfgs.append(W.prepare(x, cell, np.zeros(len(x), np.int32), 5.0))
     b = W.concat(cfgs)
-    assert b.n_rows >= 32768
+    assert b.n_rows >= 8192
     k = _module_kind("sf")
     dE = np.random.default_rng(31).normal(size=(b.n_rows, int(k.width)))
     db = B.DeviceBatch.from_batch(b, k)
