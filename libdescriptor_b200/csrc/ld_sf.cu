@@ -23,7 +23,9 @@ namespace ldb {
 namespace {
 using namespace sfc;
 
-template <bool VJP, int M2, int M3>
+// PH: 0 both sums, 2 the two-body sums only, 3 the three-body sums only
+// (large batches run 2 then 3, see launch_t)
+template <bool VJP, int M2, int M3, int PH = 0>
 __global__ void __launch_bounds__(kSFThreads, VJP ? 3 : 4)
 sf_kernel(SFDev p, RowArgs a, int per_warp_doubles, int *queue) {
     extern __shared__ double smem[];
@@ -99,7 +101,7 @@ sf_kernel(SFDev p, RowArgs a, int per_warp_doubles, int *queue) {
         const double *dE = VJP ? a.dE + (size_t)cur_row * width : nullptr;
         double gix = 0.0, giy = 0.0, giz = 0.0;
         // ---- two-body terms (g1, g2, g3)
-        if (p.n2 > 0) {
+        if (PH != 3 && p.n2 > 0) {
             double acc2[M2];
 #pragma unroll
             for (int q = 0; q < M2; ++q) acc2[q] = 0.0;
@@ -152,7 +154,7 @@ sf_kernel(SFDev p, RowArgs a, int per_warp_doubles, int *queue) {
             }
         }
         // ---- three-body terms (g4, g5)
-        if (p.n3 > 0) {
+        if (PH != 2 && p.n3 > 0) {
             double acc3[M3];
 #pragma unroll
             for (int q = 0; q < M3; ++q) acc3[q] = 0.0;
@@ -337,8 +339,20 @@ sf_kernel(SFDev p, RowArgs a, int per_warp_doubles, int *queue) {
     }
 }
 
+// Batches of at least this many rows run the two-body and the three-body
+// sums as two launches, so that each launch's hot code stays in the
+// instruction cache while the warps drift apart over hundreds of rows (the
+// rows' neighbours are staged twice; 0 disables the split)
+#ifndef LD_SF_SPLIT_ROWS
+#define LD_SF_SPLIT_ROWS 8192
+#endif
 template <bool VJP, int M2, int M3>
 int launch_t(const SFDev &p, const RowArgs &a, cudaStream_t s) {
+    if (LD_SF_SPLIT_ROWS > 0 && a.n_rows >= LD_SF_SPLIT_ROWS && p.n2 > 0 && p.n3 > 0) {
+        int rc = launch_rows_kernel(sf_kernel<VJP, M2, M3, 2>, p, a, s, VJP, "sf_kernel");
+        if (rc) return rc;
+        return launch_rows_kernel(sf_kernel<VJP, M2, M3, 3>, p, a, s, VJP, "sf_kernel");
+    }
     return launch_rows_kernel(sf_kernel<VJP, M2, M3>, p, a, s, VJP, "sf_kernel");
 }
 

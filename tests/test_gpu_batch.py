@@ -232,10 +232,12 @@ def test_torch_autograd_function(kind):
             assert abs(fd - g[a, d]) <= 1e-6 * max(1.0, abs(g[a, d])), (a, d, fd, g[a, d])
 
 
-def test_large_sf_batch_split_launches_match_per_config():
+@pytest.mark.parametrize("generic", [False, True])
+def test_large_sf_batch_split_launches_match_per_config(generic):
     """A symmetry-function batch of at least 8192 rows runs its two-body and
     three-body sums as two launches; each of its 4096-atom cells alone runs
-    the single kernel.  Both give the same descriptors and forces."""
+    the single kernel.  Both give the same descriptors and forces, for the
+    factored kernel and for the table-driven one (forced)."""
     import libdescriptor_b200 as lds
     from libdescriptor_b200 import batch as B
     from libdescriptor_b200 import workloads as W
@@ -247,6 +249,8 @@ def test_large_sf_batch_split_launches_match_per_config():
     b = W.concat(cfgs)
     assert b.n_rows >= 8192
     k = _module_kind("sf")
+    if generic:
+        B.set_tuning(k, {"sf_generic": 1})
     dE = np.random.default_rng(31).normal(size=(b.n_rows, int(k.width)))
     db = B.DeviceBatch.from_batch(b, k)
     ps = B.BatchedPass(k, db, _dev(dE, torch.float64))
