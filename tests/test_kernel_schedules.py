@@ -103,7 +103,9 @@ def test_rows_in_lanes_z_window_equals_direct_sum(J):
         for ma in range(j + 1):
             z = np.zeros(nc, complex)
             ca = c + ma
-            rem = nst % nc
+            hi = nst - 1
+            nmain = min(c, hi) + 1        # steps 0..min(c, hi): any column may be valid
+            rem = nmain % nc
             for ma2 in range(max(0, ca - j1), min(j2, ca) + 1):
                 ma1 = ca - ma2
                 ga = w[ma1, ma2]
@@ -114,13 +116,22 @@ def test_rows_in_lanes_z_window_equals_direct_sum(J):
                     x = ld(xrow + mb)
                     z += G[mb] * x * np.array(win)
                     win = [ga * ld(wrow - mb)] + win[:-1]
-                for mb0 in range(rem, nst, nc):            # rotation blocks
+                for mb0 in range(rem, nmain, nc):          # rotation blocks
                     for s in range(nc):
                         mb = mb0 + s
                         x = ld(xrow + mb)
                         for q in range(nc):
                             z[q] += G[mb, q] * x * win[(q - s + nc) % nc]
                         win[(nc - 1 - s) % nc] = ga * ld(wrow - mb)
+                for k in range(1, nc):                     # tail: steps c + k, columns q >= k
+                    mb = c + k
+                    if mb > hi:
+                        break
+                    x = ld(xrow + mb)
+                    s = k - 1
+                    for q in range(k, nc):
+                        z[q] += G[mb, q] * x * win[(q - s + nc) % nc]
+                    # the entering element (column 0) is never used again
             for q in range(nc):
                 ref = 0j
                 for ma1 in range(j1 + 1):
