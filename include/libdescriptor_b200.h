@@ -222,7 +222,8 @@ int ld_rows_work_bytes(const ld_descriptor *d, int n_rows, int vjp, size_t *byte
 #define LD_TUNE_SF_WARPS 0        /* symmetry functions: warps per CTA (1, 2, 4) */
 #define LD_TUNE_CTAS_PER_SM 1     /* per-centre kernels: resident CTA cap per SM */
 #define LD_TUNE_PAIR_GRID_MULT 2  /* bispectrum pair kernel: grid cap / (SMs x occupancy) */
-#define LD_TUNE_DYNAMIC_QUEUE 3   /* 1: centres claimed from an atomic counter   */
+#define LD_TUNE_DYNAMIC_QUEUE 3   /* centres claimed from an atomic counter: 1 on,
+                                     2 off, 0 (built-in) on for 8192+ rows     */
 #define LD_TUNE_SF_GENERIC 4      /* 1: table-driven symmetry-function kernel even
                                      when the parameter set has a factored form */
 int ld_set_tuning(ld_descriptor *d, int key, int value);

@@ -6,8 +6,9 @@ and call the per-configuration kernel once each.  Here the rows of all
 configurations sit in one device arena (the ``compute_batch`` layout: centre
 of row (c, j) is ``j + config_ptr[c]``, neighbour indices global) and one
 descriptor + VJP pass covers them all: the kernels are persistent (grid =
-SMs x resident CTAs) and, with the ``dynamic_queue`` tuning, claim centre rows
-from one global atomic counter.  ``BatchedPass.capture()`` records the pass
+SMs x resident CTAs) and claim centre rows from one global atomic counter
+(the built-in choice for batches of 8192 rows or more; the ``dynamic_queue``
+tuning forces it on (1) or off (2)).  ``BatchedPass.capture()`` records the pass
 (gradient zeroing, row-queue reset, the kernels) in a CUDA graph;
 ``replay()`` re-issues it with one call.  The per-configuration launch loop,
 the shape the reference's batch API has, is ``BatchedPass.run_per_config``.

@@ -797,7 +797,11 @@ int launch_rows(ld_descriptor *d, const RowArgs &a0, cudaStream_t s) {
     a.ctas_per_sm = d->tune[LD_TUNE_CTAS_PER_SM];
     a.pair_grid_mult = d->tune[LD_TUNE_PAIR_GRID_MULT];
     // the allocation-free entry point never takes the queue counter
-    a.dynamic_queue = a0.fused_only ? 0 : d->tune[LD_TUNE_DYNAMIC_QUEUE];
+    // the row queue: 1 always, 2 never, 0 (built-in) for batches of at least
+    // 8192 rows, whose rows of uneven cost balance better when claimed from a
+    // counter than in grid-stride order
+    const int dq = d->tune[LD_TUNE_DYNAMIC_QUEUE];
+    a.dynamic_queue = a0.fused_only ? 0 : (dq == 1 ? 1 : dq == 2 ? 0 : (a0.n_rows >= 8192 ? 1 : 0));
     a.force_generic = d->tune[LD_TUNE_SF_GENERIC] != 0;
     if (d->kind == LD_KIND_SYMMETRY_FUNCTIONS) return sf_launch(d->sf, a, s);
     return bs_launch(d->bs, a, s);
@@ -1468,7 +1472,9 @@ int ld_set_tuning(ld_descriptor *d, int key, int value) {
     if (value < 0) value = 0;
     if (key == LD_TUNE_SF_WARPS && value != 0 && value != 1 && value != 2 && value != 4)
         return fail(LD_ERR_INVALID_ARG, "LD_TUNE_SF_WARPS must be 1, 2 or 4");
-    if (key == LD_TUNE_DYNAMIC_QUEUE || key == LD_TUNE_SF_GENERIC) value = value ? 1 : 0;
+    if (key == LD_TUNE_DYNAMIC_QUEUE && value > 2)
+        return fail(LD_ERR_INVALID_ARG, "LD_TUNE_DYNAMIC_QUEUE must be 0 (built-in), 1 (on) or 2 (off)");
+    if (key == LD_TUNE_SF_GENERIC) value = value ? 1 : 0;
     std::lock_guard<std::mutex> lk(d->mu);
     d->tune[key] = value;
     return LD_OK;

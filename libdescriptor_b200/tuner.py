@@ -29,9 +29,9 @@ def candidates(kind_code: int) -> list[dict]:
     1 (bispectrum)."""
     if kind_code == 0:
         return [dict(sf_warps=w, ctas_per_sm=c, dynamic_queue=q)
-                for w, c, q in itertools.product((1, 2, 4), (0, 8), (0, 1))]
+                for w, c, q in itertools.product((1, 2, 4), (0, 8), (1, 2))]
     return [dict(ctas_per_sm=c, pair_grid_mult=m, dynamic_queue=q)
-            for c, m, q in itertools.product((0, 1), (2, 4, 8, 16), (0, 1))]
+            for c, m, q in itertools.product((0, 1), (2, 4, 8, 16), (1, 2))]
 
 
 def shape_key(device_name: str, signature: str, n_rows: int, max_neigh: int) -> str:

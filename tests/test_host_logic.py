@@ -188,7 +188,7 @@ def test_tuner_candidates_and_cache(tmp_path, monkeypatch):
     sf = tuner.candidates(0)
     bs = tuner.candidates(1)
     assert {c["sf_warps"] for c in sf} == {1, 2, 4}
-    assert {c["dynamic_queue"] for c in sf + bs} == {0, 1}
+    assert {c["dynamic_queue"] for c in sf + bs} == {1, 2}   # explicit on / off (0 is the built-in choice)
     assert {c["pair_grid_mult"] for c in bs} == {2, 4, 8, 16}
     assert tuner.shape_key("B200", "x", 1000, 30) == tuner.shape_key("B200", "x", 1024, 30)
     assert tuner.shape_key("B200", "x", 1025, 30) != tuner.shape_key("B200", "x", 1024, 30)
