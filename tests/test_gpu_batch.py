@@ -155,6 +155,10 @@ def test_tuning_rejects_bad_values():
         h.set_tuning(0, 3)     # warps per CTA must be 1, 2 or 4
     with pytest.raises(AbiError):
         h.set_tuning(9, 1)     # unknown key
+    with pytest.raises(AbiError):
+        h.set_tuning(3, 3)     # row queue: 0 built-in, 1 on, 2 off
+    h.set_tuning(3, 2)
+    assert h.get_tuning(3) == 2
 
 
 @pytest.mark.parametrize("kind", ["sf", "bs"])
