@@ -1,0 +1,54 @@
+"""GPU: the host API at megabyte sizes, with the caller's arrays in pageable
+memory (plain numpy) and in pinned memory.  At 7,999 atoms (input and result
+sizes of about a megabyte, none a round number of pages) both kinds must give
+the oracle's descriptors and gradient, and the same numbers as each other.
+"""
+import numpy as np
+import pytest
+
+from helpers import DESC_RTOL, GRAD_RTOL, assert_close
+
+pytestmark = pytest.mark.gpu
+
+
+def _pinned(a):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+
+
+@pytest.mark.parametrize("kind", ["sf24", "bs4"])
+def test_pageable_and_pinned_inputs_give_oracle_results(oracle_mod, kind):
+    import libdescriptor_b200 as lds
+    from libdescriptor_b200 import workloads as W
+    from oracle import OracleDescriptor
+
+    x, cell, sp = W.random_packing(7999, density=0.05, dmin=2.0, n_species=2, seed=31)
+    cfg = W.prepare(x, cell, sp, 5.0)
+    cm = np.full((2, 2), 5.0)
+    if kind == "sf24":
+        t, sz, p = W.sf24_params()
+        k = lds.DescriptorKind.init_descriptor(lds.AvailableDescriptors.SymmetryFunctions, ["A", "B"], "cos", 5.0,
+                                               t, sz, p)
+        o = OracleDescriptor.symmetry_functions(2, cm, t, np.asarray(sz).reshape(-1, 2), np.asarray(p, float))
+    else:
+        k = lds.DescriptorKind.init_descriptor(lds.AvailableDescriptors.Bispectrum, 0.99363, 4, 3, 0, 0.0, 1, 0,
+                                               5.0, ["A", "B"], [1.0, 0.5])
+        o = OracleDescriptor.bispectrum(0.99363, 4, 3, 0.0, 1, 0, 2, cm, [1.0, 0.5])
+    n, w = cfg.n_atoms, int(k.width)
+    dE = np.random.default_rng(32).normal(size=(n, w))
+    assert dE.nbytes >= 256 << 10 and dE.nbytes % 4096 != 0
+    assert cfg.nbl.nbytes >= 256 << 10
+    args = (cfg.species, cfg.nbl, cfg.counts, cfg.coords)
+    desc_pg, grad_pg = lds.compute_and_gradient(k, n, *args, dE)
+    desc_pn, grad_pn = lds.compute_and_gradient(k, n, *[_pinned(a) for a in args], _pinned(dE))
+    desc_o, grad_o = o.run(n, cfg.species, cfg.nbl, cfg.counts, cfg.coords, dE=dE)
+    assert_close(desc_pg, desc_o, DESC_RTOL, f"{kind} desc, pageable inputs")
+    assert_close(grad_pg, grad_o, GRAD_RTOL, f"{kind} grad, pageable inputs")
+    # the two routes agree to rounding (sums that meet in FP64 atomics vary in
+    # their order from run to run)
+    np.testing.assert_allclose(desc_pn, desc_pg, rtol=1e-13, atol=1e-13 * np.max(np.abs(desc_pg)))
+    np.testing.assert_allclose(grad_pn, grad_pg, rtol=1e-12, atol=1e-12 * np.max(np.abs(grad_pg)))
+    # forward only
+    d2 = lds.compute(k, n, *args)
+    assert_close(d2, desc_o, DESC_RTOL, f"{kind} forward-only desc, pageable inputs")
