@@ -337,6 +337,17 @@ int ld_measure_fp64_op_cost(int op, int iters, double fp64_tflops, double *flop_
 /* Number of this library's kernel launches issued so far (all descriptors). */
 long long ld_launch_count(void);
 
+/* Pinned (page-locked) host memory for results: the device writes into it at
+ * the link's rate, where a copy into fresh pageable memory runs several
+ * times slower.  Blocks are rounded up to 64 KiB; a released block is kept
+ * for reuse (up to 256 MiB in all) and handed out again for requests of
+ * between half its size and its size.  No reference counterpart: the
+ * reference computes on the host.  ld_host_alloc sets *p to NULL on failure;
+ * ld_host_free(NULL) and pointers that did not come from ld_host_alloc are
+ * ignored.  Both are thread-safe. */
+int ld_host_alloc(size_t bytes, void **p);
+void ld_host_free(void *p);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1135,6 +1135,68 @@ const char *ld_error_message(void) { return g_err.c_str(); }
 int ld_version(void) { return 10000 * 0 + 100 * 1 + 0; }
 long long ld_launch_count(void) { return g_launches.load(); }
 
+namespace {
+// Pinned result blocks: sizes by pointer, released blocks by size.  The pool
+// lives on the heap and is never destroyed, so a block released during
+// process exit (a result array freed late) finds it intact.
+struct PinPool {
+    std::mutex mu;
+    std::map<void *, size_t> size;
+    std::multimap<size_t, void *> idle;
+    size_t kept = 0;
+};
+PinPool &pin_pool() {
+    static PinPool *pool = new PinPool;
+    return *pool;
+}
+constexpr size_t kPinRound = 64u << 10, kPinKeep = 256u << 20;
+}  // namespace
+
+int ld_host_alloc(size_t bytes, void **p) {
+    if (!p) return fail(LD_ERR_INVALID_ARG, "p is NULL");
+    *p = nullptr;
+    const size_t want = ((bytes ? bytes : 1) + kPinRound - 1) / kPinRound * kPinRound;
+    PinPool &pool = pin_pool();
+    {
+        std::lock_guard<std::mutex> lk(pool.mu);
+        auto it = pool.idle.lower_bound(want);
+        if (it != pool.idle.end() && it->first / 2 <= want) {
+            *p = it->second;
+            pool.kept -= it->first;
+            pool.idle.erase(it);
+            return LD_OK;
+        }
+    }
+    void *q = nullptr;
+    const cudaError_t e = cudaHostAlloc(&q, want, cudaHostAllocPortable);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return cuda_fail(e, "cudaHostAlloc");
+    }
+    std::lock_guard<std::mutex> lk(pool.mu);
+    pool.size[q] = want;
+    *p = q;
+    return LD_OK;
+}
+
+void ld_host_free(void *p) {
+    if (!p) return;
+    PinPool &pool = pin_pool();
+    {
+        std::lock_guard<std::mutex> lk(pool.mu);
+        auto it = pool.size.find(p);
+        if (it == pool.size.end()) return;
+        if (pool.kept + it->second <= kPinKeep) {
+            pool.idle.emplace(it->second, p);
+            pool.kept += it->second;
+            return;
+        }
+        pool.size.erase(it);
+    }
+    cudaFreeHost(p);
+    cudaGetLastError();
+}
+
 static int new_handle(ld_descriptor **out) {
     if (!out) return fail(LD_ERR_INVALID_ARG, "out is NULL");
     *out = nullptr;

@@ -36,6 +36,29 @@ void check(int rc) {
     throw std::runtime_error(msg);
 }
 
+// A float64 result array.  From a quarter MiB up to 64 MiB it lives in the
+// library's pinned host blocks (returned to them when the array is freed):
+// the device writes there at the link's rate, where the copy into a fresh
+// pageable array is bound by its page faults.  Otherwise, or when no pinned
+// memory can be had, an ordinary numpy array.
+py::array_t<double> result_array(std::vector<py::ssize_t> shape) {
+    size_t n = 1;
+    for (auto e : shape) n *= (size_t)std::max<py::ssize_t>(e, 0);
+    const size_t bytes = n * sizeof(double);
+    if (bytes >= (256u << 10) && bytes <= (64u << 20)) {
+        void *p = nullptr;
+        if (ld_host_alloc(bytes, &p) == LD_OK && p) {
+            py::capsule owner(p, [](void *q) { ld_host_free(q); });
+            return py::array_t<double>(shape, static_cast<double *>(p), owner);
+        }
+    }
+    return py::array_t<double>(shape);
+}
+
+std::vector<py::ssize_t> coords_shape(const DArr &coords) {
+    return {coords.shape(0), coords.ndim() > 1 ? coords.shape(1) : (py::ssize_t)1};
+}
+
 struct Kind {
     int kind = 0;  // AvailableDescriptor
     std::string param_file;
@@ -201,7 +224,7 @@ PYBIND11_MODULE(_libdescriptor, m) {
 
     m.def("compute", [](Kind &ds, int n_atoms, IArr species, IArr neighbors, IArr number_of_neighbors, DArr coords) {
         if ((int)number_of_neighbors.size() < n_atoms) throw py::value_error("number_of_neighbors shorter than n_atoms");
-        py::array_t<double> out({n_atoms, ds.width()});
+        auto out = result_array({n_atoms, ds.width()});
         check(ld_compute(ds.get(), n_atoms, (int)(coords.size() / 3), species.data(), neighbors.data(),
                          number_of_neighbors.data(), coords.data(), out.mutable_data()));
         return out;
@@ -212,7 +235,7 @@ PYBIND11_MODULE(_libdescriptor, m) {
         const int nc = (int)n_atoms.size();
         long long tot = 0;
         for (int c = 0; c < nc; ++c) tot += n_atoms.data()[c];
-        py::array_t<double> out({(py::ssize_t)tot, (py::ssize_t)ds.width()});
+        auto out = result_array({(py::ssize_t)tot, (py::ssize_t)ds.width()});
         check(ld_compute_batch(ds.get(), nc, n_atoms.data(), config_ptr.data(), (int)(coords.size() / 3),
                                species.data(), neighbors.data(), number_of_neighbors.data(), coords.data(),
                                out.mutable_data()));
@@ -234,7 +257,7 @@ PYBIND11_MODULE(_libdescriptor, m) {
         (void)desc;  // recomputed on the device in the same pass
         if ((long long)dE_ddesc.size() < (long long)n_atoms * ds.width())
             throw py::value_error("dE_ddesc must hold n_atoms * width values");
-        py::array_t<double> out({coords.shape(0), coords.ndim() > 1 ? coords.shape(1) : (py::ssize_t)1});
+        auto out = result_array(coords_shape(coords));
         check(ld_gradient(ds.get(), n_atoms, (int)(coords.size() / 3), species.data(), neighbors.data(),
                           number_of_neighbors.data(), coords.data(), dE_ddesc.data(), out.mutable_data(), nullptr));
         return out;
@@ -259,8 +282,8 @@ PYBIND11_MODULE(_libdescriptor, m) {
                                      DArr coords, DArr dE_ddesc) {
         if ((long long)dE_ddesc.size() < (long long)n_atoms * ds.width())
             throw py::value_error("dE_ddesc must hold n_atoms * width values");
-        py::array_t<double> desc({n_atoms, ds.width()});
-        py::array_t<double> out({coords.shape(0), coords.ndim() > 1 ? coords.shape(1) : (py::ssize_t)1});
+        auto desc = result_array({n_atoms, ds.width()});
+        auto out = result_array(coords_shape(coords));
         {
             py::gil_scoped_release nogil;
             check(ld_gradient(ds.get(), n_atoms, (int)(coords.size() / 3), species.data(), neighbors.data(),
@@ -273,7 +296,7 @@ PYBIND11_MODULE(_libdescriptor, m) {
     m.def("gradient_batch", [](Kind &ds, IArr n_atoms, IArr config_ptr, IArr species, IArr neighbors,
                                IArr number_of_neighbors, DArr coords, DArr desc, DArr dE_ddesc) {
         (void)desc;
-        py::array_t<double> out({coords.shape(0), coords.ndim() > 1 ? coords.shape(1) : (py::ssize_t)1});
+        auto out = result_array(coords_shape(coords));
         check(ld_gradient_batch(ds.get(), (int)n_atoms.size(), n_atoms.data(), config_ptr.data(),
                                 (int)(coords.size() / 3), species.data(), neighbors.data(),
                                 number_of_neighbors.data(), coords.data(), dE_ddesc.data(), out.mutable_data(),
