@@ -639,9 +639,11 @@ int bs_launch(const BSDev &p, const RowArgs &a, cudaStream_t s) {
     if (per_sm < 1) per_sm = 1;
     long long grid = (long long)nsm * per_sm;
     if (a.n_rows < grid) grid = a.n_rows;
+    if (a.in_ready) LDB_CUDA(cudaStreamWaitEvent(s, a.in_ready, 0));
     kern<<<(unsigned)grid, NT, smem, s>>>(p, a, cap);
     count_launch();
     LDB_CUDA(cudaGetLastError());
+    if (a.desc_done) LDB_CUDA(cudaEventRecord(a.desc_done, s));
     return LD_OK;
 }
 

@@ -128,6 +128,10 @@ struct ld_descriptor {
     // host-API staging (grow-only)
     ldb::DevBuf species, nbl, off, coords, desc, dE, dc, centre, list, status, tmp, work;
     cudaStream_t stream = nullptr;
+    // the host API's second stream: dE's upload and the descriptors' read-back
+    // overlap the kernels that do not need them
+    cudaStream_t stream2 = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_desc = nullptr;
     std::mutex mu;
     // introspection
     std::vector<int> bs_out_j1, bs_out_j2, bs_out_j;
@@ -145,6 +149,24 @@ static int ensure_stream(ld_descriptor *d) {
     LDB_CUDA(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking));
     return LD_OK;
 }
+
+static int ensure_stream2(ld_descriptor *d) {
+    if (d->stream2 && d->ev_in && d->ev_desc) return LD_OK;
+    LDB_CUDA(cudaSetDevice(d->device));
+    if (!d->stream2) LDB_CUDA(cudaStreamCreateWithFlags(&d->stream2, cudaStreamNonBlocking));
+    if (!d->ev_in) LDB_CUDA(cudaEventCreateWithFlags(&d->ev_in, cudaEventDisableTiming));
+    if (!d->ev_desc) LDB_CUDA(cudaEventCreateWithFlags(&d->ev_desc, cudaEventDisableTiming));
+    return LD_OK;
+}
+
+// Drains the second stream when the host API returns, on every path: a copy
+// still running there must not meet the next call's buffers.
+struct DrainOnExit {
+    cudaStream_t st = nullptr;
+    ~DrainOnExit() {
+        if (st) cudaStreamSynchronize(st);
+    }
+};
 
 static int check_device() {
     int n = 0;
@@ -803,7 +825,14 @@ int launch_rows(ld_descriptor *d, const RowArgs &a0, cudaStream_t s) {
     const int dq = d->tune[LD_TUNE_DYNAMIC_QUEUE];
     a.dynamic_queue = a0.fused_only ? 0 : (dq == 1 ? 1 : dq == 2 ? 0 : (a0.n_rows >= 8192 ? 1 : 0));
     a.force_generic = d->tune[LD_TUNE_SF_GENERIC] != 0;
-    if (d->kind == LD_KIND_SYMMETRY_FUNCTIONS) return sf_launch(d->sf, a, s);
+    if (d->kind == LD_KIND_SYMMETRY_FUNCTIONS) {
+        // one fused pass: dE is read from the first kernel on, and the
+        // descriptors are final with the last
+        if (a.in_ready) LDB_CUDA(cudaStreamWaitEvent(s, a.in_ready, 0));
+        const int rc = sf_launch(d->sf, a, s);
+        if (rc == LD_OK && a.desc_done) LDB_CUDA(cudaEventRecord(a.desc_done, s));
+        return rc;
+    }
     return bs_launch(d->bs, a, s);
 }
 
@@ -904,6 +933,7 @@ static int host_pass_impl(ld_descriptor *d, HostRows &h, int n_total, const int 
         a.row_list = d->list.as<int>();
     }
     std::vector<double> onehot;
+    DrainOnExit drain;
     if (desc || !dE) {
         if ((rc = d->desc.ensure(sizeof(double) * std::max<size_t>((size_t)rows * W, 1)))) return rc;
         a.desc = d->desc.as<double>();
@@ -919,7 +949,12 @@ static int host_pass_impl(ld_descriptor *d, HostRows &h, int n_total, const int 
             LDB_CUDA(cudaMemcpyAsync(d->dE.p, onehot.data(), sizeof(double) * onehot.size(), cudaMemcpyHostToDevice, s));
             a.dc_stride = 3LL * n_total;
         } else if (rows > 0) {
-            LDB_CUDA(cudaMemcpyAsync(d->dE.p, dE, sizeof(double) * (size_t)rows * W, cudaMemcpyHostToDevice, s));
+            if ((rc = ensure_stream2(d))) return rc;
+            drain.st = d->stream2;
+            LDB_CUDA(cudaMemcpyAsync(d->dE.p, dE, sizeof(double) * (size_t)rows * W, cudaMemcpyHostToDevice,
+                                     d->stream2));
+            LDB_CUDA(cudaEventRecord(d->ev_in, d->stream2));
+            a.in_ready = d->ev_in;
         }
         LDB_CUDA(cudaMemsetAsync(d->dc.p, 0, sizeof(double) * ndc, s));
         a.dE = d->dE.as<double>();
@@ -934,7 +969,18 @@ static int host_pass_impl(ld_descriptor *d, HostRows &h, int n_total, const int 
         if ((rc = d->work.ensure(wb))) return rc;
         a.work = d->work.p;
         a.work_bytes = wb;
+        // with a gradient, the descriptors are read back on the second stream
+        // as soon as they are final (issued before the gradient's copy, which
+        // blocks the host when its destination is pageable)
+        const bool early_desc = desc && a.desc && a.in_ready;
+        if (early_desc) a.desc_done = d->ev_desc;
         if ((rc = launch_rows(d, a, s))) return rc;
+        if (early_desc) {
+            LDB_CUDA(cudaStreamWaitEvent(d->stream2, d->ev_desc, 0));
+            LDB_CUDA(cudaMemcpyAsync(desc, d->desc.p, sizeof(double) * (size_t)rows * W, cudaMemcpyDeviceToHost,
+                                     d->stream2));
+            desc = nullptr;
+        }
     }
     if (dE) {
         const size_t ndc = jac_width > 0 ? (size_t)rows * 3 * n_total : (size_t)3 * n_total;
@@ -943,6 +989,7 @@ static int host_pass_impl(ld_descriptor *d, HostRows &h, int n_total, const int 
     if (desc && a.desc && rows > 0)
         LDB_CUDA(cudaMemcpyAsync(desc, d->desc.p, sizeof(double) * (size_t)rows * W, cudaMemcpyDeviceToHost, s));
     LDB_CUDA(cudaStreamSynchronize(s));
+    if (drain.st) LDB_CUDA(cudaStreamSynchronize(drain.st));
     return read_status(d, s);
 }
 
@@ -1253,6 +1300,9 @@ int ld_create_from_file(ld_descriptor **out, const char *path, int kind) {
 int ld_destroy(ld_descriptor *d) {
     if (!d) return LD_OK;
     if (d->stream) cudaStreamDestroy(d->stream);
+    if (d->stream2) cudaStreamDestroy(d->stream2);
+    if (d->ev_in) cudaEventDestroy(d->ev_in);
+    if (d->ev_desc) cudaEventDestroy(d->ev_desc);
     delete d;
     return LD_OK;
 }

@@ -191,6 +191,11 @@ struct RowArgs {
     int pair_grid_mult = 0;            // pair-parallel gradient grid = SMs x occupancy x this
     int dynamic_queue = 0;
     bool force_generic = false;        // symmetry functions: table-driven kernel even when a grid exists
+    // host API overlap (nullable): the launches wait for in_ready before the
+    // first kernel that reads dE, and record desc_done once the descriptors
+    // are final (the bispectrum's pair-gradient kernel then still runs)
+    cudaEvent_t in_ready = nullptr;
+    cudaEvent_t desc_done = nullptr;
     // caller-provided device work space (nullable: stream-ordered allocation)
     void *work = nullptr;
     size_t work_bytes = 0;             // 1: rows claimed from an atomic counter instead of grid stride
