@@ -886,14 +886,13 @@ static int host_pass_impl(ld_descriptor *d, HostRows &h, int n_total, const int 
         return fail(LD_ERR_INVALID_ARG, "NULL input array");
     if (dE && h.n_rows > 0 && !dcoords) return fail(LD_ERR_INVALID_ARG, "d_coords is NULL");
     if (!dE && h.n_rows > 0 && !desc) return fail(LD_ERR_INVALID_ARG, "desc is NULL");
-    int rc = validate(d, h, n_total, species, nbl);
-    if (rc) return rc;
+    int rc = LD_OK;
+    if (h.n_rows == 0 && !dE) return validate(d, h, n_total, species, nbl);
     std::lock_guard<std::mutex> lk(d->mu);
     if ((rc = ensure_stream(d)) || (rc = ensure_status(d))) return rc;
     cudaStream_t s = d->stream;
     const int W = d->width;
     const int rows = jac_width > 0 ? h.n_rows * jac_width : h.n_rows;
-    if (rows == 0 && !dE) return LD_OK;
     if ((rc = d->species.ensure(sizeof(int) * std::max(n_total, 1))) || (rc = d->nbl.ensure(sizeof(int) * std::max<long long>(h.nnz, 1))) ||
         (rc = d->off.ensure(sizeof(long long) * (h.n_rows + 1))) || (rc = d->coords.ensure(sizeof(double) * 3 * std::max(n_total, 1))))
         return rc;
@@ -960,6 +959,13 @@ static int host_pass_impl(ld_descriptor *d, HostRows &h, int n_total, const int 
         a.dE = d->dE.as<double>();
         a.dcoords = d->dc.as<double>();
         if (jac_width > 0) a.desc = nullptr;
+    }
+    // the indices are checked on the host while the uploads run; no kernel
+    // is launched before they pass, and a failed check leaves no copy from
+    // the caller's arrays in flight
+    if ((rc = validate(d, h, n_total, species, nbl))) {
+        cudaStreamSynchronize(s);
+        return rc;
     }
     if (rows > 0) {
         // the kernels' work space lives in a grow-only buffer of the handle,

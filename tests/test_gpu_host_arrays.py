@@ -2,7 +2,8 @@
 memory (plain numpy) and in pinned memory.  At 7,999 atoms (input and result
 sizes of about a megabyte, none a round number of pages) both kinds must give
 the oracle's descriptors and gradient, and the same numbers as each other.
-Results of a quarter MiB and up come back in pinned host memory.
+Results of a quarter MiB and up come back in pinned host memory.  Invalid
+indices raise before any kernel runs and leave the handle usable.
 """
 import numpy as np
 import pytest
@@ -65,3 +66,40 @@ def test_pageable_and_pinned_inputs_give_oracle_results(oracle_mod, kind):
         assert_close(d3, desc_o, DESC_RTOL, f"{kind} desc, recycled result blocks")
         assert_close(g3, grad_o, GRAD_RTOL, f"{kind} grad, recycled result blocks")
         del d3, g3
+
+
+@pytest.mark.parametrize("kind", ["sf24", "bs4"])
+def test_bad_indices_raise_and_leave_the_handle_usable(oracle_mod, kind):
+    """A neighbour index outside the coordinates or a species outside the
+    descriptor's list is an invalid argument (ValueError, nothing launched);
+    the same handle then computes a valid call correctly."""
+    import libdescriptor_b200 as lds
+    from libdescriptor_b200 import workloads as W
+    from oracle import OracleDescriptor
+
+    x, cell, sp = W.random_packing(300, density=0.05, dmin=2.0, n_species=2, seed=33)
+    cfg = W.prepare(x, cell, sp, 5.0)
+    cm = np.full((2, 2), 5.0)
+    if kind == "sf24":
+        t, sz, p = W.sf24_params()
+        k = lds.DescriptorKind.init_descriptor(lds.AvailableDescriptors.SymmetryFunctions, ["A", "B"], "cos", 5.0,
+                                               t, sz, p)
+        o = OracleDescriptor.symmetry_functions(2, cm, t, np.asarray(sz).reshape(-1, 2), np.asarray(p, float))
+    else:
+        k = lds.DescriptorKind.init_descriptor(lds.AvailableDescriptors.Bispectrum, 0.99363, 4, 3, 0, 0.0, 1, 0,
+                                               5.0, ["A", "B"], [1.0, 0.5])
+        o = OracleDescriptor.bispectrum(0.99363, 4, 3, 0.0, 1, 0, 2, cm, [1.0, 0.5])
+    n, w = cfg.n_atoms, int(k.width)
+    dE = np.random.default_rng(34).normal(size=(n, w))
+    bad_nbl = cfg.nbl.copy()
+    bad_nbl[len(bad_nbl) // 2] = cfg.n_total
+    with pytest.raises(ValueError, match="neighbor_list"):
+        lds.compute_and_gradient(k, n, cfg.species, bad_nbl, cfg.counts, cfg.coords, dE)
+    bad_sp = cfg.species.copy()
+    bad_sp[n // 3] = 2
+    with pytest.raises(ValueError, match="species"):
+        lds.compute(k, n, bad_sp, cfg.nbl, cfg.counts, cfg.coords)
+    desc, grad = lds.compute_and_gradient(k, n, cfg.species, cfg.nbl, cfg.counts, cfg.coords, dE)
+    desc_o, grad_o = o.run(n, cfg.species, cfg.nbl, cfg.counts, cfg.coords, dE=dE)
+    assert_close(desc, desc_o, DESC_RTOL, f"{kind} desc after rejected calls")
+    assert_close(grad, grad_o, GRAD_RTOL, f"{kind} grad after rejected calls")
