@@ -792,8 +792,22 @@ static int make_rows(int n_rows, const int *counts, HostRows &h) {
     return LD_OK;
 }
 
-static int validate(const ld_descriptor *d, const HostRows &h, int n_total, const int *species,
-                    const int *nbl) {
+// The shapes: centre rows inside the coordinates.
+static int validate_rows(const HostRows &h, int n_total) {
+    if (!h.centre.empty()) {
+        for (int r = 0; r < h.n_rows; ++r)
+            if (h.centre[r] < 0 || h.centre[r] >= n_total)
+                return fail(LD_ERR_INVALID_ARG, "centre atom " + std::to_string(h.centre[r]) + " outside coords");
+    } else if (h.n_rows > n_total) {
+        return fail(LD_ERR_INVALID_ARG, "n_atoms exceeds the number of coordinates");
+    }
+    return LD_OK;
+}
+
+// The indices: species inside the descriptor's list, neighbours inside the
+// coordinates.
+static int validate_indices(const ld_descriptor *d, const HostRows &h, int n_total, const int *species,
+                            const int *nbl) {
     const int ns = d->kind == LD_KIND_SYMMETRY_FUNCTIONS ? d->sf.ns : d->bs.ns;
     for (int a = 0; a < n_total; ++a)
         if (species[a] < 0 || species[a] >= ns)
@@ -803,14 +817,13 @@ static int validate(const ld_descriptor *d, const HostRows &h, int n_total, cons
         if (nbl[q] < 0 || nbl[q] >= n_total)
             return fail(LD_ERR_INVALID_ARG, "neighbor_list[" + std::to_string(q) + "]=" + std::to_string(nbl[q]) +
                                                 " outside 0.." + std::to_string(n_total - 1));
-    if (!h.centre.empty()) {
-        for (int r = 0; r < h.n_rows; ++r)
-            if (h.centre[r] < 0 || h.centre[r] >= n_total)
-                return fail(LD_ERR_INVALID_ARG, "centre atom " + std::to_string(h.centre[r]) + " outside coords");
-    } else if (h.n_rows > n_total) {
-        return fail(LD_ERR_INVALID_ARG, "n_atoms exceeds the number of coordinates");
-    }
     return LD_OK;
+}
+
+static int validate(const ld_descriptor *d, const HostRows &h, int n_total, const int *species,
+                    const int *nbl) {
+    const int rc = validate_indices(d, h, n_total, species, nbl);
+    return rc ? rc : validate_rows(h, n_total);
 }
 
 int launch_rows(ld_descriptor *d, const RowArgs &a0, cudaStream_t s) {
@@ -886,8 +899,9 @@ static int host_pass_impl(ld_descriptor *d, HostRows &h, int n_total, const int 
         return fail(LD_ERR_INVALID_ARG, "NULL input array");
     if (dE && h.n_rows > 0 && !dcoords) return fail(LD_ERR_INVALID_ARG, "d_coords is NULL");
     if (!dE && h.n_rows > 0 && !desc) return fail(LD_ERR_INVALID_ARG, "desc is NULL");
-    int rc = LD_OK;
-    if (h.n_rows == 0 && !dE) return validate(d, h, n_total, species, nbl);
+    int rc = validate_rows(h, n_total);
+    if (rc) return rc;
+    if (h.n_rows == 0 && !dE) return validate_indices(d, h, n_total, species, nbl);
     std::lock_guard<std::mutex> lk(d->mu);
     if ((rc = ensure_stream(d)) || (rc = ensure_status(d))) return rc;
     cudaStream_t s = d->stream;
@@ -963,7 +977,7 @@ static int host_pass_impl(ld_descriptor *d, HostRows &h, int n_total, const int 
     // the indices are checked on the host while the uploads run; no kernel
     // is launched before they pass, and a failed check leaves no copy from
     // the caller's arrays in flight
-    if ((rc = validate(d, h, n_total, species, nbl))) {
+    if ((rc = validate_indices(d, h, n_total, species, nbl))) {
         cudaStreamSynchronize(s);
         return rc;
     }

@@ -99,6 +99,12 @@ def test_bad_indices_raise_and_leave_the_handle_usable(oracle_mod, kind):
     bad_sp[n // 3] = 2
     with pytest.raises(ValueError, match="species"):
         lds.compute(k, n, bad_sp, cfg.nbl, cfg.counts, cfg.coords)
+    # more centre rows than coordinates: rejected before any buffer is sized
+    n_big = cfg.n_total + 1
+    counts_big = np.concatenate([cfg.counts, np.zeros(n_big - n, np.int32)]).astype(np.int32)
+    dE_big = np.zeros((n_big, w))
+    with pytest.raises(ValueError, match="n_atoms exceeds"):
+        lds.compute_and_gradient(k, n_big, cfg.species, cfg.nbl, counts_big, cfg.coords, dE_big)
     desc, grad = lds.compute_and_gradient(k, n, cfg.species, cfg.nbl, cfg.counts, cfg.coords, dE)
     desc_o, grad_o = o.run(n, cfg.species, cfg.nbl, cfg.counts, cfg.coords, dE=dE)
     assert_close(desc, desc_o, DESC_RTOL, f"{kind} desc after rejected calls")
