@@ -132,6 +132,7 @@ struct ld_descriptor {
     // overlap the kernels that do not need them
     cudaStream_t stream2 = nullptr;
     cudaEvent_t ev_in = nullptr, ev_desc = nullptr;
+    int *hstatus = nullptr;   // pinned copy of the device status word
     std::mutex mu;
     // introspection
     std::vector<int> bs_out_j1, bs_out_j2, bs_out_j;
@@ -849,11 +850,7 @@ int launch_rows(ld_descriptor *d, const RowArgs &a0, cudaStream_t s) {
     return bs_launch(d->bs, a, s);
 }
 
-static int read_status(ld_descriptor *d, cudaStream_t s) {
-    if (!d->status.p) return LD_OK;
-    int st = 0;
-    LDB_CUDA(cudaMemcpyAsync(&st, d->status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
-    LDB_CUDA(cudaStreamSynchronize(s));
+static int status_error(ld_descriptor *d, cudaStream_t s, int st) {
     if (st != 0) {
         LDB_CUDA(cudaMemsetAsync(d->status.p, 0, sizeof(int), s));
         LDB_CUDA(cudaStreamSynchronize(s));
@@ -863,11 +860,25 @@ static int read_status(ld_descriptor *d, cudaStream_t s) {
     return LD_OK;
 }
 
+static int read_status(ld_descriptor *d, cudaStream_t s) {
+    if (!d->status.p) return LD_OK;
+    int st = 0;
+    LDB_CUDA(cudaMemcpyAsync(&st, d->status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    LDB_CUDA(cudaStreamSynchronize(s));
+    return status_error(d, s, st);
+}
+
 static int ensure_status(ld_descriptor *d) {
     if (d->status.p) return LD_OK;
     int rc = d->status.ensure(sizeof(int) * 4);
     if (rc) return rc;
     LDB_CUDA(cudaMemset(d->status.p, 0, sizeof(int) * 4));
+    // a pinned copy of the word, read back with a call's results (no pinned
+    // memory: read_status's own round trip instead)
+    if (!d->hstatus && cudaHostAlloc((void **)&d->hstatus, 64, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        d->hstatus = nullptr;
+    }
     return LD_OK;
 }
 
@@ -1008,9 +1019,16 @@ static int host_pass_impl(ld_descriptor *d, HostRows &h, int n_total, const int 
     }
     if (desc && a.desc && rows > 0)
         LDB_CUDA(cudaMemcpyAsync(desc, d->desc.p, sizeof(double) * (size_t)rows * W, cudaMemcpyDeviceToHost, s));
+    if (!d->hstatus) {
+        LDB_CUDA(cudaStreamSynchronize(s));
+        if (drain.st) LDB_CUDA(cudaStreamSynchronize(drain.st));
+        return read_status(d, s);
+    }
+    // the status word travels with the results: one synchronisation
+    LDB_CUDA(cudaMemcpyAsync(d->hstatus, d->status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     LDB_CUDA(cudaStreamSynchronize(s));
     if (drain.st) LDB_CUDA(cudaStreamSynchronize(drain.st));
-    return read_status(d, s);
+    return status_error(d, s, *d->hstatus);
 }
 
 static void batch_centres(int n_configs, const int *n_atoms, const int *config_ptr, std::vector<int> &c) {
@@ -1323,6 +1341,7 @@ int ld_destroy(ld_descriptor *d) {
     if (d->stream2) cudaStreamDestroy(d->stream2);
     if (d->ev_in) cudaEventDestroy(d->ev_in);
     if (d->ev_desc) cudaEventDestroy(d->ev_desc);
+    if (d->hstatus) cudaFreeHost(d->hstatus);
     delete d;
     return LD_OK;
 }
