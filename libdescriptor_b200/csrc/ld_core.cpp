@@ -810,14 +810,24 @@ static int validate_rows(const HostRows &h, int n_total) {
 static int validate_indices(const ld_descriptor *d, const HostRows &h, int n_total, const int *species,
                             const int *nbl) {
     const int ns = d->kind == LD_KIND_SYMMETRY_FUNCTIONS ? d->sf.ns : d->bs.ns;
-    for (int a = 0; a < n_total; ++a)
-        if (species[a] < 0 || species[a] >= ns)
-            return fail(LD_ERR_INVALID_ARG, "species[" + std::to_string(a) + "]=" + std::to_string(species[a]) +
-                                                " outside 0.." + std::to_string(ns - 1));
-    for (long long q = 0; q < h.nnz; ++q)
-        if (nbl[q] < 0 || nbl[q] >= n_total)
-            return fail(LD_ERR_INVALID_ARG, "neighbor_list[" + std::to_string(q) + "]=" + std::to_string(nbl[q]) +
-                                                " outside 0.." + std::to_string(n_total - 1));
+    // an unsigned compare per value folded into one flag (no early exit, so
+    // the loop vectorises); the first offender is looked for only on failure
+    auto any_outside = [](const int *v, long long n, int hi) {
+        unsigned bad = 0;
+        for (long long q = 0; q < n; ++q) bad |= (unsigned)((unsigned)v[q] >= (unsigned)hi);
+        return bad != 0;
+    };
+    if (any_outside(species, n_total, ns))
+        for (int a = 0; a < n_total; ++a)
+            if (species[a] < 0 || species[a] >= ns)
+                return fail(LD_ERR_INVALID_ARG, "species[" + std::to_string(a) + "]=" + std::to_string(species[a]) +
+                                                    " outside 0.." + std::to_string(ns - 1));
+    if (any_outside(nbl, h.nnz, n_total))
+        for (long long q = 0; q < h.nnz; ++q)
+            if (nbl[q] < 0 || nbl[q] >= n_total)
+                return fail(LD_ERR_INVALID_ARG, "neighbor_list[" + std::to_string(q) + "]=" +
+                                                    std::to_string(nbl[q]) + " outside 0.." +
+                                                    std::to_string(n_total - 1));
     return LD_OK;
 }
 
