@@ -36,7 +36,7 @@ void check(int rc) {
     throw std::runtime_error(msg);
 }
 
-// A float64 result array.  From a quarter MiB up to 64 MiB it lives in the
+// A float64 result array.  From 64 KiB up to 64 MiB it lives in the
 // library's pinned host blocks (returned to them when the array is freed):
 // the device writes there at the link's rate, where the copy into a fresh
 // pageable array is bound by its page faults.  Otherwise, or when no pinned
@@ -45,7 +45,7 @@ py::array_t<double> result_array(std::vector<py::ssize_t> shape) {
     size_t n = 1;
     for (auto e : shape) n *= (size_t)std::max<py::ssize_t>(e, 0);
     const size_t bytes = n * sizeof(double);
-    if (bytes >= (256u << 10) && bytes <= (64u << 20)) {
+    if (bytes >= (64u << 10) && bytes <= (64u << 20)) {
         void *p = nullptr;
         if (ld_host_alloc(bytes, &p) == LD_OK && p) {
             py::capsule owner(p, [](void *q) { ld_host_free(q); });

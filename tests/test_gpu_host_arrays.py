@@ -2,7 +2,7 @@
 memory (plain numpy) and in pinned memory.  At 7,999 atoms (input and result
 sizes of about a megabyte, none a round number of pages) both kinds must give
 the oracle's descriptors and gradient, and the same numbers as each other.
-Results of a quarter MiB and up come back in pinned host memory.  Invalid
+Results of 64 KiB and up come back in pinned host memory.  Invalid
 indices raise before any kernel runs and leave the handle usable.
 """
 import numpy as np
@@ -54,12 +54,13 @@ def test_pageable_and_pinned_inputs_give_oracle_results(oracle_mod, kind):
     # forward only
     d2 = lds.compute(k, n, *args)
     assert_close(d2, desc_o, DESC_RTOL, f"{kind} forward-only desc, pageable inputs")
-    # results of a quarter MiB and up come back in pinned host memory, whose
+    # results of 64 KiB and up come back in pinned host memory, whose
     # blocks are recycled when the arrays are freed: repeated calls that drop
     # their results reuse them and still return the right numbers
     import torch
 
     assert torch.from_numpy(desc_pg).is_pinned() and torch.from_numpy(d2).is_pinned()
+    assert torch.from_numpy(grad_pg).is_pinned()
     del desc_pn, grad_pn, d2
     for _ in range(3):
         d3, g3 = lds.compute_and_gradient(k, n, *args, dE)
