@@ -341,7 +341,9 @@ long long ld_launch_count(void);
  * the link's rate, where a copy into fresh pageable memory runs several
  * times slower.  Blocks are rounded up to 64 KiB; a released block is kept
  * for reuse (up to 256 MiB in all) and handed out again for requests of
- * between half its size and its size.  No reference counterpart: the
+ * between half its size and its size.  While 512 MiB are handed out and not
+ * released, a request that no kept block serves fails with LD_ERR_CAPACITY
+ * (callers then use pageable memory).  No reference counterpart: the
  * reference computes on the host.  ld_host_alloc sets *p to NULL on failure;
  * ld_host_free(NULL) and pointers that did not come from ld_host_alloc are
  * ignored.  Both are thread-safe. */

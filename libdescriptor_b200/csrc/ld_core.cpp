@@ -1238,13 +1238,14 @@ struct PinPool {
     std::mutex mu;
     std::map<void *, size_t> size;
     std::multimap<size_t, void *> idle;
-    size_t kept = 0;
+    size_t kept = 0;   // bytes of idle blocks
+    size_t out = 0;    // bytes handed out and not yet released
 };
 PinPool &pin_pool() {
     static PinPool *pool = new PinPool;
     return *pool;
 }
-constexpr size_t kPinRound = 64u << 10, kPinKeep = 256u << 20;
+constexpr size_t kPinRound = 64u << 10, kPinKeep = 256u << 20, kPinOut = 512u << 20;
 }  // namespace
 
 int ld_host_alloc(size_t bytes, void **p) {
@@ -1258,9 +1259,15 @@ int ld_host_alloc(size_t bytes, void **p) {
         if (it != pool.idle.end() && it->first / 2 <= want) {
             *p = it->second;
             pool.kept -= it->first;
+            pool.out += it->first;
             pool.idle.erase(it);
             return LD_OK;
         }
+        // callers that keep their results release nothing: past this bound
+        // each new block would be a fresh page-locking allocation, dearer
+        // than the pageable copy it saves
+        if (pool.out + want > kPinOut)
+            return fail(LD_ERR_CAPACITY, "pinned result blocks: 512 MiB handed out and not released");
     }
     void *q = nullptr;
     const cudaError_t e = cudaHostAlloc(&q, want, cudaHostAllocPortable);
@@ -1270,6 +1277,7 @@ int ld_host_alloc(size_t bytes, void **p) {
     }
     std::lock_guard<std::mutex> lk(pool.mu);
     pool.size[q] = want;
+    pool.out += want;
     *p = q;
     return LD_OK;
 }
@@ -1281,6 +1289,7 @@ void ld_host_free(void *p) {
         std::lock_guard<std::mutex> lk(pool.mu);
         auto it = pool.size.find(p);
         if (it == pool.size.end()) return;
+        pool.out -= it->second;
         if (pool.kept + it->second <= kPinKeep) {
             pool.idle.emplace(it->second, p);
             pool.kept += it->second;

@@ -110,3 +110,37 @@ def test_bad_indices_raise_and_leave_the_handle_usable(oracle_mod, kind):
     desc_o, grad_o = o.run(n, cfg.species, cfg.nbl, cfg.counts, cfg.coords, dE=dE)
     assert_close(desc, desc_o, DESC_RTOL, f"{kind} desc after rejected calls")
     assert_close(grad, grad_o, GRAD_RTOL, f"{kind} grad after rejected calls")
+
+
+def test_pinned_result_blocks_are_bounded_and_recycled():
+    """ld_host_alloc / ld_host_free through the C ABI: blocks of 200 MiB are
+    handed out until 512 MiB would be outstanding (then LD_ERR_CAPACITY, and
+    the module falls back to pageable arrays); a released block is kept and
+    handed out again for a request of the same size."""
+    import ctypes as C
+
+    import libdescriptor_b200  # noqa: F401  (loads the library and a CUDA context)
+    from abi import Abi
+
+    L = Abi.lib()
+    L.ld_host_alloc.argtypes = [C.c_size_t, C.POINTER(C.c_void_p)]
+    L.ld_host_alloc.restype = C.c_int
+    L.ld_host_free.argtypes = [C.c_void_p]
+    L.ld_host_free.restype = None
+    size = 200 << 20
+    a, b, c = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    assert L.ld_host_alloc(size, C.byref(a)) == 0 and a.value
+    assert L.ld_host_alloc(size, C.byref(b)) == 0 and b.value
+    try:
+        assert L.ld_host_alloc(size, C.byref(c)) == 3      # LD_ERR_CAPACITY
+        assert not c.value
+        L.ld_host_free(b)
+        assert L.ld_host_alloc(size, C.byref(c)) == 0 and c.value == b.value
+        # the memory is usable host memory
+        C.memset(c.value, 7, 4096)
+        assert C.string_at(c.value, 4)[0] == 7
+    finally:
+        L.ld_host_free(a)
+        L.ld_host_free(c)
+    L.ld_host_free(None)
+    L.ld_host_free(C.c_void_p(12345))                      # not from ld_host_alloc: ignored
