@@ -20,6 +20,8 @@
 #ifndef LIBDESCRIPTOR_B200_H_
 #define LIBDESCRIPTOR_B200_H_
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -79,6 +81,19 @@ int ld_create_bispectrum(ld_descriptor **out, double rfac0, int twojmax,
  * src/SymmetryFunctions.cpp:266-407, Bispectrum::initFromFile
  * src/Bispectrum.cpp:852-1007). */
 int ld_create_from_file(ld_descriptor **out, const char *path, int kind);
+
+/* Reads and checks a parameter file on the host only (no device, no
+ * tables): writes what the file defines, with the reference's reading
+ * quirks applied, as "key = values" lines into text[capacity] (NUL
+ * terminated; *length = bytes needed including the NUL).  Keys: kind,
+ * n_species, species, cutoff_matrix, then type_codes, sizes, params
+ * (symmetry functions) or rfac0, twojmax, diagonalstyle, rmin0,
+ * switch_flag, bzero_flag, weights (bispectrum).  No reference counterpart
+ * (its initFromFile builds the descriptor directly); lets a caller validate
+ * a file without a GPU.  LD_ERR_PARSE on a malformed file, LD_ERR_CAPACITY
+ * when text is too small (it then holds a truncated copy). */
+int ld_describe_parameter_file(const char *path, int kind, char *text, size_t capacity,
+                               size_t *length);
 
 int ld_destroy(ld_descriptor *d);
 int ld_width(const ld_descriptor *d, int *width);   /* DescriptorKind::width */
@@ -266,7 +281,11 @@ int ld_stage_request(int n_atoms, int n_total, long long nnz, int width,
  * Limit: n_rows <= 262144 per call (larger requests return LD_ERR_CAPACITY).
  * d_coords is accumulated into; the call waits for `stream` and returns any
  * device-side status (LD_ERR_CAPACITY when a row exceeds max_neigh).  All
- * calls share the array: calls that overlap on the GPU race on it. */
+ * calls share the array: calls that overlap on the GPU race on it.  The
+ * current device must be the descriptor's (else LD_ERR_INVALID_ARG), and, as
+ * with ld_gradient_dev, the caller keeps every index inside the coordinates:
+ * the number of coordinate rows is not passed, so no device-side index check
+ * runs. */
 int ld_gradient_counts_dev_noalloc(ld_descriptor *d, int n_rows, const int *row_centre,
                                    const int *species, const int *neighbor_list,
                                    const int *number_of_neighs, int max_neigh,
@@ -336,6 +355,19 @@ int ld_measure_fp64_op_cost(int op, int iters, double fp64_tflops, double *flop_
 
 /* Number of this library's kernel launches issued so far (all descriptors). */
 long long ld_launch_count(void);
+
+/* Number of device allocations this library has requested so far: growth of
+ * a handle's buffers (cudaMalloc) and stream-ordered scratch taken from the
+ * library's per-device pool.  No reference counterpart (the reference
+ * allocates host memory only); lets a caller check that a call allocated
+ * nothing. */
+long long ld_alloc_count(void);
+
+/* Fault injection for tests of the out-of-memory path (no reference
+ * counterpart): the k-th device allocation from now (k >= 1) fails with
+ * LD_ERR_OOM, as a failed cudaMalloc would; k = 0 disarms.  Host-side only:
+ * nothing is asked of the device, and the handle stays usable afterwards. */
+int ld_fail_next_allocation(int k);
 
 /* Pinned (page-locked) host memory for results: the device writes into it at
  * the link's rate, where a copy into fresh pageable memory runs several

@@ -39,10 +39,27 @@ int cuda_fail(cudaError_t e, const char *what) {
 }
 void count_launch(int n) { g_launches += n; }
 
+// Device allocations of the library (grow-only buffers and the scratch
+// pool), and the test hook that makes the k-th next one fail.
+static std::atomic<long long> g_allocs{0};
+static std::atomic<int> g_fail_in{0};
+int count_alloc() {
+    ++g_allocs;
+    int k = g_fail_in.load();
+    while (k > 0) {
+        if (g_fail_in.compare_exchange_weak(k, k - 1)) {
+            if (k == 1) return fail(LD_ERR_OOM, "device allocation failed (injected by ld_fail_next_allocation)");
+            break;
+        }
+    }
+    return LD_OK;
+}
+
 int DevBuf::ensure(size_t n) {
     if (n <= bytes && p) return LD_OK;
     release();
     size_t want = n < 256 ? 256 : n;
+    if (int rc = count_alloc()) return rc;
     cudaError_t e = cudaMalloc(&p, want);
     if (e != cudaSuccess) {
         p = nullptr;
@@ -144,6 +161,8 @@ struct ld_descriptor {
 
 namespace ldb {
 
+int handle_device(const ld_descriptor *d) { return d->device; }
+
 static int ensure_stream(ld_descriptor *d) {
     if (d->stream) return LD_OK;
     LDB_CUDA(cudaSetDevice(d->device));
@@ -160,8 +179,9 @@ static int ensure_stream2(ld_descriptor *d) {
     return LD_OK;
 }
 
-// Drains the second stream when the host API returns, on every path: a copy
-// still running there must not meet the next call's buffers.
+// Drains a stream when the host API returns, on every path: a copy still
+// running there must neither meet the next call's buffers nor read the
+// caller's arrays after the call has returned.
 struct DrainOnExit {
     cudaStream_t st = nullptr;
     ~DrainOnExit() {
@@ -931,6 +951,10 @@ static int host_pass_impl(ld_descriptor *d, HostRows &h, int n_total, const int 
     if ((rc = d->species.ensure(sizeof(int) * std::max(n_total, 1))) || (rc = d->nbl.ensure(sizeof(int) * std::max<long long>(h.nnz, 1))) ||
         (rc = d->off.ensure(sizeof(long long) * (h.n_rows + 1))) || (rc = d->coords.ensure(sizeof(double) * 3 * std::max(n_total, 1))))
         return rc;
+    // from the first upload on, every return waits for the handle's stream:
+    // an error return must not leave copies from the caller's arrays running
+    DrainOnExit drain_s;
+    drain_s.st = s;
     LDB_CUDA(cudaMemcpyAsync(d->species.p, species, sizeof(int) * n_total, cudaMemcpyHostToDevice, s));
     if (h.nnz) LDB_CUDA(cudaMemcpyAsync(d->nbl.p, nbl, sizeof(int) * h.nnz, cudaMemcpyHostToDevice, s));
     LDB_CUDA(cudaMemcpyAsync(d->off.p, h.off.data(), sizeof(long long) * (h.n_rows + 1), cudaMemcpyHostToDevice, s));
@@ -996,12 +1020,9 @@ static int host_pass_impl(ld_descriptor *d, HostRows &h, int n_total, const int 
         if (jac_width > 0) a.desc = nullptr;
     }
     // the indices are checked on the host while the uploads run; no kernel
-    // is launched before they pass, and a failed check leaves no copy from
-    // the caller's arrays in flight
-    if ((rc = validate_indices(d, h, n_total, species, nbl))) {
-        cudaStreamSynchronize(s);
-        return rc;
-    }
+    // is launched before they pass (the guards above drain both streams on
+    // this and every other error return)
+    if ((rc = validate_indices(d, h, n_total, species, nbl))) return rc;
     if (rows > 0) {
         // the kernels' work space lives in a grow-only buffer of the handle,
         // so repeated calls allocate nothing
@@ -1031,12 +1052,14 @@ static int host_pass_impl(ld_descriptor *d, HostRows &h, int n_total, const int 
         LDB_CUDA(cudaMemcpyAsync(desc, d->desc.p, sizeof(double) * (size_t)rows * W, cudaMemcpyDeviceToHost, s));
     if (!d->hstatus) {
         LDB_CUDA(cudaStreamSynchronize(s));
+        drain_s.st = nullptr;
         if (drain.st) LDB_CUDA(cudaStreamSynchronize(drain.st));
         return read_status(d, s);
     }
     // the status word travels with the results: one synchronisation
     LDB_CUDA(cudaMemcpyAsync(d->hstatus, d->status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     LDB_CUDA(cudaStreamSynchronize(s));
+    drain_s.st = nullptr;
     if (drain.st) LDB_CUDA(cudaStreamSynchronize(drain.st));
     return status_error(d, s, *d->hstatus);
 }
@@ -1123,17 +1146,33 @@ static int parse_species(LineReader &lr, int n_species, std::vector<std::string>
     return LD_OK;
 }
 
-static int parse_file_impl(ld_descriptor *d, const char *path, int kind);
+// What a parameter file defines, before any device table is built.
+struct ParsedFile {
+    int kind = -1, ns = 0;
+    std::vector<std::string> species;
+    std::vector<double> cutoff;                 // ns x ns
+    std::vector<int> codes, sizes;              // symmetry functions
+    std::vector<double> params;
+    double rfac0 = 0, rmin0 = 0;                // bispectrum
+    int twojmax = 0, style = 0, sw = 0, bz = 0;
+    std::vector<double> weights;
+};
 
-static int parse_file(ld_descriptor *d, const char *path, int kind) {
+static int parse_file_impl(ParsedFile &pf, const char *path, int kind);
+
+static int parse_file(ParsedFile &pf, const char *path, int kind) {
     try {
-        return parse_file_impl(d, path, kind);
+        return parse_file_impl(pf, path, kind);
     } catch (const std::exception &e) {
         return fail(LD_ERR_PARSE, std::string("parameter file: ") + e.what());
     }
 }
 
-static int parse_file_impl(ld_descriptor *d, const char *path, int kind) {
+static int parse_file_impl(ParsedFile &pf, const char *path, int kind) {
+    if (!path) return fail(LD_ERR_INVALID_ARG, "path is NULL");
+    if (kind != LD_KIND_SYMMETRY_FUNCTIONS && kind != LD_KIND_BISPECTRUM)
+        return fail(LD_ERR_INVALID_KIND, "descriptor kind " + std::to_string(kind) +
+                                             " is not supported (SOAP and Xi are out of scope)");
     LineReader lr;
     lr.f.open(path);
     if (!lr.f.is_open()) return fail(LD_ERR_PARSE, std::string("Could not open file: ") + path);
@@ -1143,10 +1182,9 @@ static int parse_file_impl(ld_descriptor *d, const char *path, int kind) {
     std::vector<std::string> sv;
     if (!lr.next(line) || !tok_strings(line, 1, sv)) return fail(LD_ERR_PARSE, "parameter file: cutoff type");
     if (!lr.next(line) || !tok_ints(line, 1, iv) || iv[0] <= 0) return fail(LD_ERR_PARSE, "parameter file: number of species");
-    const int ns = iv[0];
-    std::vector<std::string> species;
-    std::vector<double> cutoff;
-    int rc = parse_species(lr, ns, species, cutoff);
+    pf.kind = kind;
+    pf.ns = iv[0];
+    int rc = parse_species(lr, pf.ns, pf.species, pf.cutoff);
     if (rc) return rc;
     if (kind == LD_KIND_SYMMETRY_FUNCTIONS) {
         // src/SymmetryFunctions.cpp:326-406.  The parameter vector is shared
@@ -1155,7 +1193,6 @@ static int parse_file_impl(ld_descriptor *d, const char *path, int kind) {
         if (!lr.next(line) || !tok_ints(line, 1, iv)) return fail(LD_ERR_PARSE, "parameter file: number of types");
         const int nt = iv[0];
         std::vector<std::string> names;
-        std::vector<int> codes, sizes;
         std::vector<double> acc;
         std::map<std::string, std::vector<double>> per_type;
         std::map<std::string, std::pair<int, int>> type_sizes;
@@ -1172,7 +1209,6 @@ static int parse_file_impl(ld_descriptor *d, const char *path, int kind) {
         }
         if (!lr.next(line)) return fail(LD_ERR_PARSE, "parameter file: normalize flag");
         if (!lr.next(line) || !tok_ints(line, 1, iv)) return fail(LD_ERR_PARSE, "parameter file: descriptor size");
-        std::vector<double> params;
         for (auto &nm : names) {
             int code = 0;
             if (nm == "g1") code = 1;
@@ -1182,39 +1218,67 @@ static int parse_file_impl(ld_descriptor *d, const char *path, int kind) {
             else if (nm == "g5") code = 5;
             if (!code) return fail(LD_ERR_PARSE, "parameter file: unknown symmetry function " + nm);
             const auto sz = type_sizes[nm];
-            codes.push_back(code);
-            sizes.push_back(sz.first);
-            sizes.push_back(sz.second);
+            pf.codes.push_back(code);
+            pf.sizes.push_back(sz.first);
+            pf.sizes.push_back(sz.second);
             const auto &src = per_type[nm];
             const size_t need = (size_t)sz.first * sz.second;
             if (src.size() < need) return fail(LD_ERR_PARSE, "parameter file: too few parameters");
-            params.insert(params.end(), src.begin(), src.begin() + need);
+            pf.params.insert(pf.params.end(), src.begin(), src.begin() + need);
         }
-        return build_sf(d, ns, cutoff.data(), (int)codes.size(), codes.data(), sizes.data(), params.data());
+        return LD_OK;
     }
-    if (kind == LD_KIND_BISPECTRUM) {
-        // src/Bispectrum.cpp:909-1006: jmax (doubled), rfac0, diagonalstyle,
-        // rmin0, switch flag, bzero flag, one weight per species
-        int jmax, style, sw, bz;
-        double rfac0, rmin0;
-        if (!lr.next(line) || !tok_ints(line, 1, iv)) return fail(LD_ERR_PARSE, "parameter file: jmax");
-        jmax = iv[0];
-        if (!lr.next(line) || !tok_doubles(line, 1, dv)) return fail(LD_ERR_PARSE, "parameter file: rfac0");
-        rfac0 = dv[0];
-        if (!lr.next(line) || !tok_ints(line, 1, iv)) return fail(LD_ERR_PARSE, "parameter file: diagonalstyle");
-        style = iv[0];
-        if (!lr.next(line) || !tok_doubles(line, 1, dv)) return fail(LD_ERR_PARSE, "parameter file: rmin0");
-        rmin0 = dv[0];
-        if (!lr.next(line) || !tok_ints(line, 1, iv)) return fail(LD_ERR_PARSE, "parameter file: switch flag");
-        sw = iv[0];
-        if (!lr.next(line) || !tok_ints(line, 1, iv)) return fail(LD_ERR_PARSE, "parameter file: bzero flag");
-        bz = iv[0];
-        if (!lr.next(line) || !tok_doubles(line, (int)species.size(), dv)) return fail(LD_ERR_PARSE, "parameter file: weights");
-        std::vector<double> w(ns, 0.0);
-        for (int k = 0; k < ns && k < (int)dv.size(); ++k) w[k] = dv[k];
-        return build_bs(d, rfac0, 2 * jmax, style, rmin0, sw, bz, ns, cutoff.data(), w.data());
+    // src/Bispectrum.cpp:909-1006: jmax (doubled), rfac0, diagonalstyle,
+    // rmin0, switch flag, bzero flag, one weight per species
+    if (!lr.next(line) || !tok_ints(line, 1, iv)) return fail(LD_ERR_PARSE, "parameter file: jmax");
+    pf.twojmax = 2 * iv[0];
+    if (!lr.next(line) || !tok_doubles(line, 1, dv)) return fail(LD_ERR_PARSE, "parameter file: rfac0");
+    pf.rfac0 = dv[0];
+    if (!lr.next(line) || !tok_ints(line, 1, iv)) return fail(LD_ERR_PARSE, "parameter file: diagonalstyle");
+    pf.style = iv[0];
+    if (!lr.next(line) || !tok_doubles(line, 1, dv)) return fail(LD_ERR_PARSE, "parameter file: rmin0");
+    pf.rmin0 = dv[0];
+    if (!lr.next(line) || !tok_ints(line, 1, iv)) return fail(LD_ERR_PARSE, "parameter file: switch flag");
+    pf.sw = iv[0];
+    if (!lr.next(line) || !tok_ints(line, 1, iv)) return fail(LD_ERR_PARSE, "parameter file: bzero flag");
+    pf.bz = iv[0];
+    if (!lr.next(line) || !tok_doubles(line, (int)pf.species.size(), dv)) return fail(LD_ERR_PARSE, "parameter file: weights");
+    pf.weights.assign(pf.ns, 0.0);
+    for (int k = 0; k < pf.ns && k < (int)dv.size(); ++k) pf.weights[k] = dv[k];
+    return LD_OK;
+}
+
+static int build_parsed(ld_descriptor *d, const ParsedFile &pf) {
+    if (pf.kind == LD_KIND_SYMMETRY_FUNCTIONS)
+        return build_sf(d, pf.ns, pf.cutoff.data(), (int)pf.codes.size(), pf.codes.data(), pf.sizes.data(),
+                        pf.params.data());
+    return build_bs(d, pf.rfac0, pf.twojmax, pf.style, pf.rmin0, pf.sw, pf.bz, pf.ns, pf.cutoff.data(),
+                    pf.weights.data());
+}
+
+// "key = values" text of a parsed file (ld_describe_parameter_file)
+static std::string describe_parsed(const ParsedFile &pf) {
+    std::ostringstream o;
+    o.precision(17);
+    auto list = [&o](const char *key, const auto &v) {
+        o << key << " =";
+        for (const auto &x : v) o << ' ' << x;
+        o << '\n';
+    };
+    o << "kind = " << pf.kind << '\n' << "n_species = " << pf.ns << '\n';
+    list("species", pf.species);
+    list("cutoff_matrix", pf.cutoff);
+    if (pf.kind == LD_KIND_SYMMETRY_FUNCTIONS) {
+        list("type_codes", pf.codes);
+        list("sizes", pf.sizes);
+        list("params", pf.params);
+    } else {
+        o << "rfac0 = " << pf.rfac0 << '\n' << "twojmax = " << pf.twojmax << '\n' << "diagonalstyle = " << pf.style
+          << '\n' << "rmin0 = " << pf.rmin0 << '\n' << "switch_flag = " << pf.sw << '\n' << "bzero_flag = " << pf.bz
+          << '\n';
+        list("weights", pf.weights);
     }
-    return fail(LD_ERR_INVALID_KIND, "descriptor kind " + std::to_string(kind) + " is not supported (SOAP and Xi are out of scope)");
+    return o.str();
 }
 
 }  // namespace ldb
@@ -1229,6 +1293,12 @@ extern "C" {
 const char *ld_error_message(void) { return g_err.c_str(); }
 int ld_version(void) { return 10000 * 0 + 100 * 1 + 0; }
 long long ld_launch_count(void) { return g_launches.load(); }
+long long ld_alloc_count(void) { return g_allocs.load(); }
+int ld_fail_next_allocation(int k) {
+    if (k < 0) return fail(LD_ERR_INVALID_ARG, "ld_fail_next_allocation: k < 0");
+    g_fail_in.store(k);
+    return LD_OK;
+}
 
 namespace {
 // Pinned result blocks: sizes by pointer, released blocks by size.  The pool
@@ -1268,16 +1338,19 @@ int ld_host_alloc(size_t bytes, void **p) {
         // than the pageable copy it saves
         if (pool.out + want > kPinOut)
             return fail(LD_ERR_CAPACITY, "pinned result blocks: 512 MiB handed out and not released");
+        // reserved before the allocation, so concurrent callers cannot pass
+        // the bound together
+        pool.out += want;
     }
     void *q = nullptr;
     const cudaError_t e = cudaHostAlloc(&q, want, cudaHostAllocPortable);
+    std::lock_guard<std::mutex> lk(pool.mu);
     if (e != cudaSuccess) {
+        pool.out -= want;
         cudaGetLastError();
         return cuda_fail(e, "cudaHostAlloc");
     }
-    std::lock_guard<std::mutex> lk(pool.mu);
     pool.size[q] = want;
-    pool.out += want;
     *p = q;
     return LD_OK;
 }
@@ -1341,17 +1414,38 @@ int ld_create_bispectrum(ld_descriptor **out, double rfac0, int twojmax, int dia
 }
 
 int ld_create_from_file(ld_descriptor **out, const char *path, int kind) {
-    if (!path) return fail(LD_ERR_INVALID_ARG, "path is NULL");
-    if (kind != LD_KIND_SYMMETRY_FUNCTIONS && kind != LD_KIND_BISPECTRUM)
-        return fail(LD_ERR_INVALID_KIND, "descriptor kind " + std::to_string(kind) + " is not supported (SOAP and Xi are out of scope)");
-    int rc = new_handle(out);
+    if (!out) return fail(LD_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    ParsedFile pf;
+    int rc = parse_file(pf, path, kind);
     if (rc) return rc;
-    rc = parse_file(*out, path, kind);
+    rc = new_handle(out);
+    if (rc) return rc;
+    try {
+        rc = build_parsed(*out, pf);
+    } catch (const std::bad_alloc &) {
+        rc = fail(LD_ERR_OOM, "host allocation failed");
+    }
     if (rc) {
         delete *out;
         *out = nullptr;
     }
     return rc;
+}
+
+int ld_describe_parameter_file(const char *path, int kind, char *text, size_t capacity, size_t *length) {
+    ParsedFile pf;
+    int rc = parse_file(pf, path, kind);
+    if (rc) return rc;
+    const std::string t = describe_parsed(pf);
+    if (length) *length = t.size() + 1;
+    if (text && capacity > 0) {
+        const size_t n = std::min(capacity - 1, t.size());
+        std::memcpy(text, t.data(), n);
+        text[n] = '\0';
+        if (n < t.size()) return fail(LD_ERR_CAPACITY, "ld_describe_parameter_file: text buffer too small");
+    }
+    return LD_OK;
 }
 
 int ld_destroy(ld_descriptor *d) {
@@ -1428,6 +1522,8 @@ static int gradient_params_impl(ld_descriptor *d, int n_atoms, int n_total, cons
         (rc = d->dE.ensure(sizeof(double) * std::max<size_t>((size_t)n_atoms * W, 1))) ||
         (rc = d->dc.ensure(sizeof(double) * (std::max(n_params, 1) + (bs ? 3 * (size_t)std::max(n_total, 1) : 0)))))
         return rc;
+    DrainOnExit drain_s;   // no copy from the caller's arrays outlives an error return
+    drain_s.st = s;
     if (n_total) LDB_CUDA(cudaMemcpyAsync(d->species.p, species, sizeof(int) * n_total, cudaMemcpyHostToDevice, s));
     if (h.nnz) LDB_CUDA(cudaMemcpyAsync(d->nbl.p, neighbor_list, sizeof(int) * h.nnz, cudaMemcpyHostToDevice, s));
     LDB_CUDA(cudaMemcpyAsync(d->off.p, h.off.data(), sizeof(long long) * (h.n_rows + 1), cudaMemcpyHostToDevice, s));

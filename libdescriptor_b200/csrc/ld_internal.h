@@ -32,6 +32,12 @@ enum DeviceStatus : int {
 
 // Launch accounting (all kernels of the library).
 void count_launch(int n = 1);
+// Allocation accounting: every device allocation of the library (grow-only
+// buffers, the stream-ordered scratch pool) calls this first; it returns
+// LD_ERR_OOM when ld_fail_next_allocation armed a failure for this one.
+int count_alloc();
+// The device a descriptor handle was created on.
+int handle_device(const ld_descriptor *d);
 
 // ------------------------------------------------------------- device buf
 struct DevBuf {
@@ -216,12 +222,6 @@ struct RowArgs {
 constexpr int kZTileA = LD_ZTILE_A;
 constexpr int kZTileB = LD_ZTILE_B;
 
-// 1: the twojmax-specialised path runs U (per centre), Z/B/Y (rows in
-// lanes) and the pair gradient as three kernels; 0: the per-centre kernel
-// computes U, Z, B and Y together
-#ifndef LD_BS_SPLIT
-#define LD_BS_SPLIT 1
-#endif
 // warps of the rows-in-lanes Z kernel's CTA (32 rows per CTA)
 #ifndef LD_ZWARPS
 #define LD_ZWARPS 16
@@ -236,10 +236,12 @@ inline size_t bs_smemZ_bytes(const BSDev &p, bool with_g = false) {
     return (size_t)(p.J + 1 + p.nU + p.J / 2 + 1) * 32 * 16 + (size_t)32 * (p.nbslot > 0 ? p.nbslot : 1) * 8 +
            (with_g ? (size_t)p.nzg * 8 + (size_t)p.ntrip * 32 * 8 : 0);
 }
-// the split form runs where its Z kernel fits one SM's shared memory; the
-// column weights and the rows' betaj join the U block there when they fit
-// too
-inline bool bs_split(const BSDev &p) { return LD_BS_SPLIT != 0 && bs_smemZ_bytes(p) <= 227 * 1024; }
+// The twojmax-specialised path runs U (per centre), Z/B/Y (rows in lanes)
+// and the pair gradient as three kernels (the split form) where its Z kernel
+// fits one SM's shared memory; otherwise (2J = 10) the per-centre kernel
+// computes U, Z, B and Y together.  The column weights and the rows' betaj
+// join the U block in shared memory when they fit too.
+inline bool bs_split(const BSDev &p) { return bs_smemZ_bytes(p) <= 227 * 1024; }
 inline bool bs_split_gshared(const BSDev &p) { return bs_smemZ_bytes(p, true) <= 227 * 1024; }
 
 // warps of the twojmax-specialised per-centre bispectrum CTA (4..8): enough

@@ -13,7 +13,9 @@
 // all calls and keeps the last call's contents; the status word is cleared
 // at the start of every call.  Calls whose work overlaps on the GPU (two
 // streams, two host threads) race on it: issue them on one stream or
-// serialise them.
+// serialise them.  Like ld_gradient_dev, the call does not know the number
+// of coordinate rows, so the caller keeps every centre and neighbour index
+// inside the coordinates (no device-side index check runs).
 #include <mutex>
 
 #include "ld_internal.h"
@@ -37,9 +39,14 @@ void *g_base[kMaxDevices] = {nullptr};
 
 // Device address of g_scratch for the current device (looked up once per
 // device: host code only holds a stand-in symbol, never a device address).
-int scratch_base(void **out) {
+// The current device must be the handle's: its parameter tables live there.
+int scratch_base(const ld_descriptor *d, void **out) {
     int dev = 0;
     LDB_CUDA(cudaGetDevice(&dev));
+    if (dev != ldb::handle_device(d))
+        return ldb::fail(LD_ERR_INVALID_ARG, "ld_gradient_counts_dev_noalloc: the current device (" +
+                                                 std::to_string(dev) + ") is not the descriptor's device (" +
+                                                 std::to_string(ldb::handle_device(d)) + ")");
     if (dev < 0 || dev >= kMaxDevices) return ldb::fail(LD_ERR_INVALID_ARG, "device ordinal too large");
     std::lock_guard<std::mutex> lk(g_mu);
     if (!g_base[dev]) {
@@ -75,7 +82,7 @@ extern "C" int ld_gradient_counts_dev_noalloc(ld_descriptor *d, int n_rows, cons
     if (tmp_need > tmp_have)
         return fail(LD_ERR_CAPACITY, "ld_gradient_counts_dev_noalloc: prefix-sum work space does not fit");
     void *base = nullptr;
-    int rc = scratch_base(&base);
+    int rc = scratch_base(d, &base);
     if (rc) return rc;
     cudaStream_t s = (cudaStream_t)stream;
     char *b = static_cast<char *>(base);
@@ -105,6 +112,6 @@ extern "C" int ld_gradient_counts_dev_noalloc(ld_descriptor *d, int n_rows, cons
     LDB_CUDA(cudaMemcpyAsync(&st, status, sizeof(int), cudaMemcpyDeviceToHost, s));
     LDB_CUDA(cudaStreamSynchronize(s));
     if (st == kDevCapacity) return fail(LD_ERR_CAPACITY, "a centre has more neighbours than max_neigh");
-    if (st != 0) return fail(LD_ERR_INVALID_ARG, "a neighbour or centre index lies outside the coordinates");
+    if (st != 0) return fail(LD_ERR_INVALID_ARG, "the kernels raised device status " + std::to_string(st));
     return LD_OK;
 }

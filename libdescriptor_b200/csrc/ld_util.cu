@@ -90,6 +90,7 @@ int pool_alloc(void **p, size_t bytes, cudaStream_t s) {
         }
         pool = pools[dev];
     }
+    if (int rc = count_alloc()) return rc;
     LDB_CUDA(cudaMallocFromPoolAsync(p, bytes ? bytes : 1, pool, s));
     return LD_OK;
 }

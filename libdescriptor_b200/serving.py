@@ -44,7 +44,9 @@ import numpy as np
 class Ring:
     """FIFO allocator of contiguous ranges in [0, cap): a range never wraps
     past the end (the tail left unused at a wrap is reclaimed when the range
-    before it is freed).  Ranges are freed in allocation order."""
+    before it is freed).  Ranges are freed in allocation order (``free``);
+    ``release`` frees one out of order (a cancelled request), and its space
+    comes back once every older range has been freed."""
 
     def __init__(self, cap: int):
         if cap <= 0:
@@ -52,6 +54,7 @@ class Ring:
         self.cap = int(cap)
         self.head = 0
         self.live: collections.deque = collections.deque()   # (start, size)
+        self.dead: set = set()                               # released, not yet reclaimed
 
     def alloc(self, n: int):
         """Start of a free range of n >= 1 elements, or None."""
@@ -80,12 +83,25 @@ class Ring:
         self.head = start + n
         return start
 
+    def _reclaim(self) -> None:
+        while self.live and self.live[0][0] in self.dead:
+            self.dead.discard(self.live.popleft()[0])
+        if not self.live:
+            self.head = 0
+
     def free(self, start: int) -> None:
+        self._reclaim()
         if not self.live or self.live[0][0] != start:
             raise RuntimeError("ring ranges must be freed in allocation order")
         self.live.popleft()
-        if not self.live:
-            self.head = 0
+        self._reclaim()
+
+    def release(self, start: int) -> None:
+        """Free a live range out of allocation order."""
+        if not any(s == start for s, _ in self.live) or start in self.dead:
+            raise RuntimeError(f"ring range at {start} is not live")
+        self.dead.add(start)
+        self._reclaim()
 
     @property
     def used(self) -> int:
@@ -111,7 +127,9 @@ class Request:
     dE: np.ndarray              # (n_atoms, width) f64
     arrival: float = 0.0
     max_neigh: int = -1
-    # filled by the scheduler
+    # filled by the scheduler; state: new -> pending -> admitted -> launched
+    # -> done, or cancelled (from new, pending or admitted)
+    state: str = "new"
     slots: tuple | None = None  # (row0, atom0, entry0)
     staged: object = None
     admitted_at: float = 0.0
@@ -193,11 +211,13 @@ class Scheduler:
         self.admitted = {k: collections.deque() for k in caps}
         self.inflight = {k: collections.deque() for k in caps}
         self.completed: list = []
+        self.cancelled: list = []
         self._out_pending: list = []   # output ranges released at the next poll
         self.n_batches = 0
         self.admission_waits = 0
         self.batch_rows: list = []
         self.batch_reqs: list = []
+        self.batch_lanes: list = []
 
     # -- admission ------------------------------------------------------
     def submit(self, req: Request) -> None:
@@ -206,7 +226,29 @@ class Scheduler:
             raise ValueError(f"request {req.rid} ({req.n_atoms} atoms) exceeds the lane's whole HBM budget")
         if req.n_atoms > min(self.max_batch_rows, self.out[req.lane].cap):
             raise ValueError(f"request {req.rid} has more rows than one batch holds")
+        req.state = "pending"
         self.pending[req.lane].append(req)
+
+    def cancel(self, req: Request) -> bool:
+        """Withdraw a request that is not on the GPU yet: a pending one leaves
+        its queue; an admitted one (inputs staged, not launched) also gives
+        back its ring space.  Returns False for a launched or finished
+        request, which completes as usual."""
+        if req.state == "new":
+            req.state = "cancelled"
+            self.cancelled.append(req)
+            return True
+        for q in (self.pending.get(req.lane, ()), self.admitted.get(req.lane, ())):
+            for i, r in enumerate(q):
+                if r is req:
+                    del q[i]
+                    if req.state == "admitted":
+                        for ring, start in zip(self.rings[req.lane], req.slots):
+                            ring.release(start)
+                    req.state = "cancelled"
+                    self.cancelled.append(req)
+                    return True
+        return False
 
     def _try_admit(self, req: Request) -> bool:
         rr, ra, re = self.rings[req.lane]
@@ -247,6 +289,7 @@ class Scheduler:
                     break
                 q.popleft()
                 req.admitted_at = now
+                req.state = "admitted"
                 self.backend.stage(req)
                 self.admitted[k].append(req)
                 rows += req.n_atoms
@@ -273,8 +316,9 @@ class Scheduler:
         out0 = self.out[k].alloc(rows)
         if out0 is None:
             return None
-        for _ in reqs:
+        for req in reqs:
             q.popleft()
+            req.state = "launched"
         return BatchPlan(k, reqs, row0, rows, mx, out0)
 
     def launch(self) -> int:
@@ -289,6 +333,7 @@ class Scheduler:
                 self.n_batches += 1
                 self.batch_rows.append(plan.n_rows)
                 self.batch_reqs.append(len(plan.reqs))
+                self.batch_lanes.append(k)
                 n += 1
         return n
 
@@ -306,6 +351,7 @@ class Scheduler:
                 self.backend.finish(plan)
                 for req in plan.reqs:
                     req.done_at = now
+                    req.state = "done"
                     done.append(req)
                 self._retire(plan)
         self.completed.extend(done)
@@ -484,6 +530,12 @@ class ServingEngine:
             req.grad = ln.out_grad[o + k:o + k + req.n_atoms].numpy()
 
     # -- driving ------------------------------------------------------------
+    def cancel(self, req: Request) -> bool:
+        """Withdraw a request that has not been launched (``Scheduler.cancel``);
+        callable from ``serve``'s ``on_done`` callback.  A cancelled request
+        gets no results and counts as finished for ``serve``."""
+        return self.sched.cancel(req)
+
     def check_status(self) -> None:
         for ln in self.lanes.values():
             self._ext._sync_status(ln.kind, ln.s_comp.cuda_stream)
@@ -502,12 +554,14 @@ class ServingEngine:
         n = len(requests)
         done = 0
         sched = self.sched
-        while done < n:
+        c0 = len(sched.cancelled)
+        while done + len(sched.cancelled) - c0 < n:
             now = self.clock()
             while nxt < n and arr[order[nxt]] <= now:
                 req = requests[order[nxt]]
                 req.arrival = float(arr[order[nxt]])
-                sched.submit(req)
+                if req.state != "cancelled":
+                    sched.submit(req)
                 nxt += 1
             for req in sched.poll(now):
                 if keep_results:
@@ -520,12 +574,14 @@ class ServingEngine:
             sched.launch()
         self.torch.cuda.synchronize()
         self.check_status()
-        lat = np.array([r.done_at - r.arrival for r in requests])
-        atoms = int(sum(r.n_atoms for r in requests))
+        served = [r for r in requests if r.state == "done"]
+        lat = np.array([r.done_at - r.arrival for r in served]) if served else np.zeros(1)
+        atoms = int(sum(r.n_atoms for r in served))
         t_first = float(arr.min()) if n else 0.0
-        t_last = max(r.done_at for r in requests) if n else 0.0
+        t_last = max(r.done_at for r in served) if served else 0.0
         span = max(t_last - t_first, 1e-9)
-        return {"requests": n, "atoms": atoms, "seconds": span, "atoms_per_s": atoms / span,
+        return {"requests": len(served), "cancelled": n - len(served), "atoms": atoms, "seconds": span,
+                "atoms_per_s": atoms / span,
                 "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
                 "batches": sched.n_batches, "mean_batch_rows": float(np.mean(sched.batch_rows)) if sched.batch_rows else 0.0,
                 "max_batch_requests": int(max(sched.batch_reqs)) if sched.batch_reqs else 0,
@@ -588,6 +644,31 @@ def packing_pool(n_pool: int, n_min: int = 16, n_max: int = 32768, density: floa
         x, cell, sp = Wk.random_packing(int(n), density=density, dmin=dmin, n_species=2, seed=seed * 1000 + i)
         pool.append(Wk.prepare(x, cell, sp, cutoff))
     return pool
+
+
+def request_stream(n_req: int, widths: dict, mix: dict, n_min: int = 16, n_max: int = 32768,
+                   density: float = 0.05, dmin: float = 2.0, cutoff: float = 5.0, seed: int = 0,
+                   source=None, grads=None, first: int = 0, last: int | None = None, device=None) -> list:
+    """Requests first .. last-1 of the served stream (``synth.stream_requests``):
+    per request its own log-uniform atom count, lane and periodic two-species
+    packing, ghosts and neighbour lists built on the device when one is given
+    (``workloads.prepare_dev``, identical to the host builder's lists) else on
+    the host, and a run of N(0, 1) dL/d(desc) rows."""
+    from . import synth
+    from . import workloads as Wk
+
+    if device is not None:
+        def prep(x, cell, sp, rc):
+            return Wk.prepare_dev(x, cell, sp, rc, device=device).to_host(cell)
+    else:
+        prep = Wk.prepare
+    reqs = []
+    for i, lane, cfg, dE in synth.stream_requests(n_req, widths, mix, prep, n_min, n_max, density, dmin, cutoff,
+                                                  seed, source, grads, first, last):
+        r = Request(i, lane, cfg.n_atoms, cfg.coords, cfg.species, cfg.image, cfg.counts, cfg.nbl, dE)
+        r.cfg = cfg
+        reqs.append(r)
+    return reqs
 
 
 def make_requests(pool: list, n_req: int, widths: dict, mix: dict, seed: int = 0) -> list:

@@ -27,7 +27,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "libldoracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libldref.so")
-REFERENCE_SRC = "/root/reference"
+# the reference source tree (its path on the build machine; override with
+# LDB200_REFERENCE_SRC)
+REFERENCE_SRC = os.environ.get("LDB200_REFERENCE_SRC", "/root/reference")
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
@@ -40,7 +42,7 @@ def build(with_ref: bool | None = None) -> None:
         with_ref = os.path.isdir(os.path.join(REFERENCE_SRC, "src"))
     if with_ref:
         targets.append("ref")
-    subprocess.check_call(["make", "-s", "-C", HERE] + targets)
+    subprocess.check_call(["make", "-s", "-C", HERE, "REF=" + REFERENCE_SRC] + targets)
 
 
 def _i32(a):
@@ -172,6 +174,8 @@ class Reference(_Lib):
         L.ref_bs_new.restype = C.c_void_p
         L.ref_bs_new.argtypes = [C.c_double, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int,
                                  C.c_int, C.c_int, _dp, _dp]
+        L.ref_from_file.restype = C.c_void_p
+        L.ref_from_file.argtypes = [C.c_char_p, C.c_int]
         L.ref_free.argtypes = [C.c_void_p]
         L.ref_width.argtypes = [C.c_void_p]
         L.ref_compute.argtypes = [C.c_void_p, C.c_int, _ip, _ip, _ip, _ip, _ip, _dp, _dp,
@@ -247,6 +251,16 @@ class ReferenceDescriptor:
         codes = _i32([int(t.lower().lstrip("g")) for t in types])
         h = L.ref_sf_new(int(n_species), _f64(cutoff_matrix).ravel(), len(codes), codes,
                          _i32(sizes).ravel(), _f64(params).ravel())
+        return cls(h, L.ref_width(h))
+
+    @classmethod
+    def from_file(cls, path, kind):
+        """The reference's parameter-file constructors (kind 0: symmetry
+        functions, 1: bispectrum)."""
+        L = Reference.lib()
+        h = L.ref_from_file(os.fsencode(path), int(kind))
+        if not h:
+            raise ValueError(f"the reference could not read {path}")
         return cls(h, L.ref_width(h))
 
     @classmethod

@@ -46,9 +46,24 @@ struct RefKind {
     double rfac0 = 0, rmin0 = 0;
     int twojmax = 0, style = 3, use_shared = 0, switch_flag = 1, bzero_flag = 0;
     std::vector<double> weights;
+    // parameter-file construction (SymmetryFunctions(std::string&),
+    // src/SymmetryFunctions.cpp:262-407; Bispectrum(std::string&),
+    // src/Bispectrum.cpp:848-1007) when set
+    std::string file;
     std::vector<Descriptor::DescriptorKind *> inst;
 
     Descriptor::DescriptorKind *make() {
+        if (!file.empty()) {
+            std::string f = file;
+            if (kind == 0) {
+                auto *sf = new SymmetryFunctions(f);
+                sf->descriptor_kind = Descriptor::KindSymmetryFunctions;
+                return sf;
+            }
+            auto *bs = new Bispectrum(f);
+            bs->descriptor_kind = Descriptor::KindBispectrum;
+            return bs;
+        }
         if (kind == 0) {
             auto *sf = new SymmetryFunctions(&species, &cutoff_function, cutoff_matrix.data(),
                                              &types, &sizes, &params);
@@ -99,6 +114,22 @@ void *ref_sf_new(int n_species, const double *cutoff_matrix, int n_types,
     }
     k->params.assign(params, params + np);
     k->get(0);
+    return k;
+}
+
+// A reference descriptor built from a parameter file (kind 0 = symmetry
+// functions, 1 = bispectrum); NULL when the reference's reader throws.
+void *ref_from_file(const char *path, int kind) {
+    auto *k = new RefKind;
+    k->kind = kind;
+    k->file = path;
+    try {
+        k->get(0);
+    } catch (const std::exception &) {
+        k->inst.clear();
+        delete k;
+        return nullptr;
+    }
     return k;
 }
 

@@ -49,11 +49,15 @@ class Abi:
             L = C.CDLL(LIB)
             L.ld_error_message.restype = C.c_char_p
             L.ld_launch_count.restype = C.c_longlong
+            L.ld_alloc_count.restype = C.c_longlong
+            L.ld_fail_next_allocation.argtypes = [C.c_int]
             L.ld_create_symmetry_functions.argtypes = [C.POINTER(C.c_void_p), C.c_int, _dp, C.c_int,
                                                        _ip, _ip, _dp]
             L.ld_create_bispectrum.argtypes = [C.POINTER(C.c_void_p), C.c_double, C.c_int, C.c_int,
                                                C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, _dp, _dp]
             L.ld_create_from_file.argtypes = [C.POINTER(C.c_void_p), C.c_char_p, C.c_int]
+            L.ld_describe_parameter_file.argtypes = [C.c_char_p, C.c_int, C.c_char_p, C.c_size_t,
+                                                     C.POINTER(C.c_size_t)]
             L.ld_destroy.argtypes = [C.c_void_p]
             L.ld_width.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
             L.ld_kind.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
@@ -125,6 +129,30 @@ class Abi:
         h = C.c_void_p()
         cls.check(cls.lib().ld_create_from_file(C.byref(h), path.encode(), int(kind)))
         return Handle(h)
+
+
+def describe_parameter_file(path, kind):
+    """ld_describe_parameter_file as a dict of numpy arrays / scalars."""
+    L = Abi.lib()
+    n = C.c_size_t(0)
+    Abi.check(L.ld_describe_parameter_file(path.encode(), int(kind), None, 0, C.byref(n)))
+    buf = C.create_string_buffer(n.value)
+    Abi.check(L.ld_describe_parameter_file(path.encode(), int(kind), buf, n.value, C.byref(n)))
+    out = {}
+    for line in buf.value.decode().splitlines():
+        key, _, val = line.partition(" = ")
+        toks = val.split()
+        if key == "species":
+            out[key] = toks
+        elif key in ("kind", "n_species", "twojmax", "diagonalstyle", "switch_flag", "bzero_flag"):
+            out[key] = int(toks[0])
+        elif key in ("type_codes", "sizes"):
+            out[key] = np.array([int(t) for t in toks], dtype=np.int32)
+        elif key in ("rfac0", "rmin0"):
+            out[key] = float(toks[0])
+        else:
+            out[key] = np.array([float(t) for t in toks])
+    return out
 
 
 class Handle:

@@ -120,3 +120,15 @@ def test_no_device_is_an_error_not_a_fallback():
     with pytest.raises(RuntimeError, match="no CUDA device"):
         lds.DescriptorKind.init_descriptor(lds.AvailableDescriptors.Bispectrum, 0.99363, 8, 3, 0, 0.0,
                                            1, 0, 5.0, ["Si"], [1.0])
+
+
+def test_allocation_fault_injection_is_host_side():
+    """ld_fail_next_allocation arms a host-side failure of the library's k-th
+    next device allocation (the GPU tests drive the failure itself); arming
+    and disarming touch no device."""
+    L = Abi.lib()
+    n0 = L.ld_alloc_count()
+    assert L.ld_fail_next_allocation(-1) == 2          # LD_ERR_INVALID_ARG
+    assert L.ld_fail_next_allocation(3) == 0
+    assert L.ld_fail_next_allocation(0) == 0           # disarmed
+    assert L.ld_alloc_count() == n0

@@ -129,6 +129,67 @@ def test_admission_waits_for_memory_and_batches_continuously():
     assert all(ring.used == 0 for rings in sch.rings.values() for ring in rings)
 
 
+def test_ring_release_out_of_order_reclaims_after_older_ranges():
+    r = S.Ring(12)
+    a, b, c = r.alloc(4), r.alloc(4), r.alloc(4)
+    r.release(b)                       # middle range: space held until a is freed
+    assert r.alloc(1) is None
+    with pytest.raises(RuntimeError):
+        r.release(b)                   # already released
+    r.free(a)                          # a and the released b come back together
+    assert [s for s, _ in r.live] == [c]
+    assert r.alloc(8) == 0
+    r.release(c)
+    r.free(0)
+    assert r.used == 0 and r.alloc(12) == 0
+
+
+def test_ring_random_release_never_overlaps():
+    rng = np.random.default_rng(3)
+    ring = S.Ring(50)
+    for _ in range(4000):
+        live = [s for s, _ in ring.live if s not in ring.dead]
+        u = rng.random()
+        if live and u < 0.25:
+            ring.free(ring.live[0][0]) if ring.live[0][0] not in ring.dead else None
+        elif live and u < 0.45:
+            ring.release(live[int(rng.integers(len(live)))])
+        else:
+            ring.alloc(int(rng.integers(1, 12)))
+        occ = _occupied(ring)
+        assert occ.max(initial=0) <= 1
+
+
+def test_cancel_pending_and_admitted_requests():
+    caps = {"sf": S.LaneCaps(rows=60, atoms=180, entries=240)}
+    dev = FakeDevice()
+    sch = S.Scheduler(caps, dev, max_batch_rows=40, depth=1, out_rows=80)
+    reqs = [_req(i, "sf", 10) for i in range(10)]
+    for r in reqs:
+        sch.submit(r)
+    sch.admit(0.0)                     # 6 admitted (60 rows), 4 pending
+    sch.launch()                       # depth 1: one batch of 4 requests (40 rows) launched
+    assert [r.state for r in reqs[:4]] == ["launched"] * 4
+    assert [r.state for r in reqs[4:6]] == ["admitted"] * 2 and reqs[6].state == "pending"
+    assert not sch.cancel(reqs[0])     # on the GPU: completes as usual
+    assert sch.cancel(reqs[4])         # admitted: its ring space is released
+    assert sch.cancel(reqs[7])         # pending: leaves the queue
+    assert not sch.cancel(reqs[7])
+    late = _req(99, "sf", 10)
+    assert sch.cancel(late) and late.state == "cancelled"   # before submission
+    while not sch.idle():
+        dev.release_all()
+        sch.step(1.0)
+    done = sorted(r.rid for r in sch.completed)
+    assert done == [0, 1, 2, 3, 5, 6, 8, 9]
+    assert [r.rid for r in sch.cancelled] == [4, 7, 99]
+    assert reqs[4].desc is None and reqs[7].desc is None
+    # every batch still covers contiguous rows, and all ring space came back
+    for p in dev.launched:
+        assert [r.slots[0] for r in p.reqs] == [p.row0 + 10 * i for i in range(len(p.reqs))]
+    assert all(ring.used == 0 for rings in sch.rings.values() for ring in rings)
+
+
 def test_oversized_request_is_rejected_up_front():
     caps = {"sf": S.LaneCaps(rows=10, atoms=30, entries=40)}
     sch = S.Scheduler(caps, FakeDevice(), max_batch_rows=8, out_rows=16)
@@ -291,3 +352,34 @@ def test_stage_request_rejects_bad_indices(bad):
         counts = [2, 0, 2]             # does not add up to nnz
     rc, *_ = _stage(n, nt, nbl, counts, image)
     assert rc == 2, Abi.lib().ld_error_message().decode()   # LD_ERR_INVALID_ARG
+
+
+# ------------------------------------------------------- served stream
+def test_stream_requests_are_fresh_periodic_packings():
+    """Every request of the served stream has its own log-uniform atom count
+    and its own periodic packing: minimum distance d_min under the request's
+    own periodicity, density 0.05 A^-3; request i is rebuilt alone from
+    (seed, i)."""
+    from scipy.spatial import cKDTree
+
+    from libdescriptor_b200 import synth
+
+    src = synth.PackingSource(n_base=1, base_atoms=4096, seed=2)
+    widths = {"sf": 24, "bs": 55}
+    sizes, lanes = synth.stream_draws(400, {"sf": 0.7, "bs": 0.3}, n_max=4096, seed=2)
+    assert len(set(sizes.tolist())) > 200 and sizes.min() >= 16 and sizes.max() <= 4096
+    assert 0.6 < lanes.count("sf") / 400 < 0.8
+    reqs = S.request_stream(12, widths, {"sf": 0.7, "bs": 0.3}, n_max=4096, seed=2, source=src)
+    for r in reqs:
+        L = float(r.cfg.cell[0, 0])
+        x = r.coords[:r.n_atoms]
+        assert np.all((x >= 0) & (x < L))
+        d, _ = cKDTree(x, boxsize=L).query(x, k=2)
+        assert d[:, 1].min() >= 2.0 - 1e-9
+        assert abs(r.n_atoms - sizes[r.rid]) <= 4 * np.sqrt(sizes[r.rid]) + 4
+        assert r.dE.shape == (r.n_atoms, widths[r.lane])
+        assert r.counts.shape == (r.n_atoms,) and r.nbl.shape == (int(r.counts.sum()),)
+    again = S.request_stream(8, widths, {"sf": 0.7, "bs": 0.3}, n_max=4096, seed=2, source=src, first=7)[0]
+    assert again.rid == 7
+    np.testing.assert_array_equal(again.coords, reqs[7].coords)
+    np.testing.assert_array_equal(again.dE, reqs[7].dE)
