@@ -5,21 +5,34 @@
 
 Workloads (seeded synthetic inputs; the reference names no dataset):
 
-  serve     (default) the served mixed stream: periodic two-species random
-            packings (0.05 A^-3, d_min 2 A, rc 5 A) with log-uniform atom
-            counts in [16, 32768], 70% 24-d symmetry functions / 30%
-            bispectrum 2J=8, desc + VJP vs N(0,1) upstream, Poisson arrivals.
-            A step is 200 requests.  value: the batched resident pass over
-            each step's requests (inputs in HBM); e2e: the continuous-batching
-            server, host arrays in and out, at the top arrival rate, beside
-            the plain per-call path (one compute_and_gradient per request) on
-            the same stream; p50/p99 latency at 1k / 10k / 50k requests/s.
+  serve     (default) the served mixed stream of 20,000 requests: each request
+            draws its own atom count log-uniformly from [16, 32768] and its own
+            periodic two-species random packing (0.05 A^-3, d_min 2 A, rc 5 A);
+            70% 24-d symmetry functions / 30% bispectrum 2J=8, desc + VJP vs
+            N(0,1) upstream, Poisson arrivals.  value: the batched resident pass
+            over steps of 200 requests (inputs in HBM); e2e: the
+            continuous-batching server over the whole stream, host arrays in and
+            out, beside the plain per-call path (one compute_and_gradient per
+            request) on the same stream, p50/p99 of both at 1k / 10k / 50k
+            requests/s.
   batch512  512 strained, jittered Si diamond supercells n_i ~ U{1..6}, each
             with 24-d symmetry functions and bispectrum 2J=6, desc + VJP: one
             persistent launch per descriptor under a CUDA graph (autotuned
             launch shape) vs the per-configuration launch loop.
   bs8       8192-atom two-species packing, bispectrum 2J=8, desc + VJP
   sf24      4096-atom Si diamond 8x8x8 (jitter 0.1 A), 24-d symmetry functions
+
+After the timed regions the CPU leg runs the oracle on a bounded sample of
+the same inputs (the baseline rate) and checks the GPU results of that sample
+against it (descriptors 1e-10, gradients 1e-8 relative); a failed check
+stops the benchmark.
+
+--impl reference: the reference-side CPU path of the same workload on all
+host cores (desc + VJP by the oracle's analytic adjoint, since the
+reference's Enzyme gradient cannot be built offline; the reference's own C++
+forward from oracle/_ref timed beside it).  Its inputs are built by the same
+generators (synth.py, loaded by file path) and the reference's own
+neighbour-list builder, so that process loads nothing of this library.
 
 Multi-GPU (torchrun): replicas only -- every rank runs its own independent
 work (the path has no exchange step); value = all ranks' atoms / max time.
@@ -34,6 +47,7 @@ import subprocess
 import sys
 import threading
 import time
+from dataclasses import dataclass, field
 
 import numpy as np
 
@@ -41,7 +55,6 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "desc+VJP atoms/s, 1 B200: served batch vs plain call; p50/p99 ms @≤1e-10 rel"
-from libdescriptor_b200.replicas import replica_throughput  # noqa: E402
 # DRAM bytes (read + write) per centre atom of the dominant kernels, from one
 # ncu capture each (profiles/, cold caches): bispectrum 2J=8 pass (U kernel
 # bsA<8,0,1> 1.41 MB, Z kernel bsZ 41.50 MB -- of which the 37.4 MB U blocks
@@ -52,15 +65,106 @@ from libdescriptor_b200.replicas import replica_throughput  # noqa: E402
 DRAM_BYTES_PER_ATOM = {"bs8": (1.414656e6 + 41.50528e6 + 21.975296e6) / 8192, "sf24": 1.747968e6 / 4096}
 BS_KERNELS = "bsA_kernel<8,0,1> (U) + bsZ_kernel<8,1,1> (Z, B, Y) + bsR_kernel<8> (pair gradient)"
 RATES = (1000.0, 10000.0, 50000.0)
+N_STREAM = 20000
 REQ_PER_STEP = 200
 MIX = {"sf": 0.7, "bs": 0.3}
+DESC_RTOL, GRAD_RTOL = 1e-10, 1e-8
+
+
+def _synth():
+    """synth.py loaded by file path: importing the package would load its
+    native extension, which the reference arm must not."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("ldb200_synth", os.path.join(ROOT, "libdescriptor_b200", "synth.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+@dataclass
+class HostCfg:
+    """One configuration in the reference's input layout (host arrays)."""
+
+    n_atoms: int
+    coords: np.ndarray
+    species: np.ndarray
+    image: np.ndarray
+    counts: np.ndarray
+    nbl: np.ndarray
+    cell: np.ndarray = field(default=None)
+
+    @property
+    def n_total(self) -> int:
+        return int(self.coords.shape[0])
+
+
+def ref_prepare(x, cell, species, cutoff, pbc=(1, 1, 1)):
+    """Ghosts and full neighbour lists from the reference's own builder
+    (nbl_create_paddings / nbl_build, compiled from its sources into
+    oracle/_ref): the reference arm's inputs, identical to this library's
+    builder's."""
+    from oracle import Reference
+
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    species = np.ascontiguousarray(species, dtype=np.int32)
+    n = x.shape[0]
+    pc, ps, pi = Reference.create_paddings(cutoff, np.asarray(cell), list(pbc), x, species)
+    allx = np.ascontiguousarray(np.concatenate([x, pc]))
+    need = np.zeros(allx.shape[0], np.int32)
+    need[:n] = 1
+    counts, nbl = Reference.neighbor_list(allx, cutoff, need, n)
+    image = np.concatenate([np.arange(n, dtype=np.int32), pi.astype(np.int32)])
+    return HostCfg(n, allx, np.concatenate([species, ps]).astype(np.int32), image, counts.astype(np.int32),
+                   nbl.astype(np.int32), np.asarray(cell))
+
+
+def rel_err(x, ref):
+    """max |x - ref| / max(|ref|, 1e-3 * column scale) (the tests' rule)."""
+    x = np.asarray(x, dtype=np.float64)
+    ref = np.asarray(ref, dtype=np.float64)
+    if ref.size == 0:
+        return 0.0
+    r2 = ref.reshape(ref.shape[0], -1)
+    x2 = x.reshape(r2.shape)
+    den = np.maximum(np.abs(r2), 1e-3 * np.max(np.abs(r2), axis=0, keepdims=True))
+    den = np.where(den == 0, 1.0, den)
+    if not np.all(np.isfinite(x2)):
+        return float("inf")
+    return float(np.max(np.abs(x2 - r2) / den))
+
+
+def fold(grad, n_atoms, image):
+    out = np.array(grad[:n_atoms], dtype=np.float64, copy=True)
+    if grad.shape[0] > n_atoms:
+        for d in range(3):
+            out[:, d] += np.bincount(image[n_atoms:], weights=grad[n_atoms:, d], minlength=n_atoms)[:n_atoms]
+    return out
+
+
+class Parity:
+    """Running maximum of the GPU-vs-oracle errors of a bench's sample."""
+
+    def __init__(self):
+        self.n, self.atoms, self.ed, self.eg = 0, 0, 0.0, 0.0
+
+    def add(self, what, desc, desc_ref, grad=None, grad_ref=None):
+        ed = rel_err(desc, desc_ref)
+        eg = rel_err(grad, grad_ref) if grad is not None else 0.0
+        if not (ed <= DESC_RTOL and eg <= GRAD_RTOL):
+            raise RuntimeError(f"parity check failed for {what}: descriptors {ed:.3e}, gradient {eg:.3e}")
+        self.n += 1
+        self.atoms += int(np.asarray(desc).shape[0])
+        self.ed, self.eg = max(self.ed, ed), max(self.eg, eg)
+
+    def summary(self, against):
+        return {"checked": self.n, "centres": self.atoms, "desc_max_rel": self.ed, "grad_max_rel": self.eg,
+                "bars": {"desc": DESC_RTOL, "grad": GRAD_RTOL}, "against": against}
 
 
 # --------------------------------------------------------------- specs
 def sf24_spec(species):
-    from libdescriptor_b200 import workloads as W
-
-    t, sz, p = W.sf24_params()
+    t, sz, p = _synth().sf24_params()
     return dict(kind="sf", types=t, sizes=sz, params=p, cutoff=5.0, species=list(species))
 
 
@@ -69,25 +173,45 @@ def bs_spec(J, species, weights):
                 species=list(species), weights=list(weights))
 
 
-def make_workload(name: str, seed: int):
+def gpu_prepare(x, cell, species, cutoff, pbc=(1, 1, 1)):
     from libdescriptor_b200 import workloads as W
 
+    return W.prepare(x, cell, species, cutoff, pbc)
+
+
+def make_workload(name: str, seed: int, prepare=gpu_prepare):
+    """The single-configuration workloads; ``prepare`` builds ghosts and
+    neighbour lists (this library's builder, or the reference's in the
+    reference arm: the lists are identical)."""
+    sy = _synth()
     if name == "bs8":
-        x, cell, sp = W.random_packing(8192, density=0.05, dmin=2.0, n_species=2, seed=seed)
-        cfg = W.prepare(x, cell, sp, 5.0)
+        x, cell, sp = sy.random_packing(8192, density=0.05, dmin=2.0, n_species=2, seed=seed)
+        cfg = prepare(x, cell, sp, 5.0)
         spec = bs_spec(8, ["A", "B"], [1.0, 0.5])
         desc = {"workload": "bispectrum_2J8_random_packing_8192", "atoms": 8192, "twojmax": 8, "width": 55,
                 "species": 2, "density": 0.05, "cutoff": 5.0, "box_side": float(cell[0, 0])}
     elif name == "sf24":
-        x, cell = W.diamond_cell(8, 8, 8, jitter=0.1, seed=seed)
+        x, cell = sy.diamond_cell(8, 8, 8, jitter=0.1, seed=seed)
         sp = np.zeros(len(x), np.int32)
-        cfg = W.prepare(x, cell, sp, 5.0)
+        cfg = prepare(x, cell, sp, 5.0)
         spec = sf24_spec(["Si"])
         desc = {"workload": "symmetry_functions_24_diamond_8x8x8", "atoms": 4096, "width": 24, "cutoff": 5.0}
     else:
         raise SystemExit(f"unknown workload {name}")
     desc["mean_neighbours"] = float(cfg.counts.mean())
     return cfg, spec, desc
+
+
+def diamond_cells(n_configs=512, seed=1, prepare=gpu_prepare, n_max=6, strain=0.03, jitter=0.1, cutoff=5.0):
+    """The 512-cell batch (the same draws as libdescriptor_b200.batch.diamond_batch)."""
+    sy = _synth()
+    rng = np.random.default_rng(seed)
+    cfgs = []
+    for _ in range(n_configs):
+        n1, n2, n3 = (int(v) for v in rng.integers(1, n_max + 1, 3))
+        x, cell = sy.diamond_cell(n1, n2, n3, jitter=jitter, strain=strain, seed=int(rng.integers(1 << 31)))
+        cfgs.append(prepare(x, cell, np.zeros(len(x), np.int32), cutoff))
+    return cfgs
 
 
 def make_descriptor(spec):
@@ -196,35 +320,39 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------- CPU legs
-def cpu_rate(spec, cfgs, budget_s=10.0, threads=None):
-    """Oracle desc+VJP atoms/s (all host threads) on a bounded sample: whole
-    configurations of ``cfgs`` in order until about budget_s of work."""
+def oracle_sample(spec, cfgs, budget_s=10.0, threads=None, dEs=None, seed=7):
+    """Oracle desc+VJP on all host threads over a bounded sample: whole
+    configurations of ``cfgs`` in order until about budget_s of work (the
+    last one may be cut to its first rows).  dEs[i]: the upstream gradient
+    of cfgs[i] (default: seeded N(0, 1)).  Returns (atoms/s, atoms, threads,
+    [(i, desc, unfolded gradient)] of the configurations done whole)."""
     ora = make_oracle(spec)
     threads = threads or os.cpu_count() or 1
-    rng = np.random.default_rng(7)
-
-    def run(cfg, nrows):
-        dE = rng.normal(size=(nrows, ora.width))
-        t0 = time.perf_counter()
-        ora.run(np.array([nrows], np.int32), cfg.species, cfg.nbl, cfg.counts[:nrows], cfg.coords, dE=dE,
-                n_configs=1, config_ptr=np.array([0], np.int32), n_threads=threads)
-        return time.perf_counter() - t0
-
-    atoms, secs = 0, 0.0
-    for cfg in cfgs:
+    rng = np.random.default_rng(seed)
+    atoms, secs, whole = 0, 0.0, []
+    for i, cfg in enumerate(cfgs):
         n = cfg.n_atoms
         if secs > 0 and atoms > 0:
             # cap the last configuration so the sample stays near the budget
-            rate = atoms / secs
-            n = int(min(n, max(16, (budget_s - secs) * rate)))
-        secs += run(cfg, n)
+            n = int(min(n, max(16, (budget_s - secs) * atoms / secs)))
+        dE = (dEs[i] if dEs is not None else rng.normal(size=(cfg.n_atoms, ora.width)))[:n]
+        t0 = time.perf_counter()
+        d, g = ora.run(np.array([n], np.int32), cfg.species, cfg.nbl, cfg.counts[:n], cfg.coords, dE=dE,
+                       n_configs=1, config_ptr=np.array([0], np.int32), n_threads=threads)
+        secs += time.perf_counter() - t0
         atoms += n
+        if n == cfg.n_atoms:
+            whole.append((i, d, g))
         if secs >= budget_s:
             break
-    return atoms / secs, atoms, threads
+    return atoms / secs, atoms, threads, whole
 
 
-def reference_forward_rate(spec, cfg, budget_s=4.0, threads=None):
+def reference_forward_rate(spec, cfgs, budget_s=4.0, threads=None):
+    """The reference's own C++ forward (SymmetryFunctions::compute /
+    Bispectrum::compute from oracle/_ref) on all host threads over whole
+    configurations of ``cfgs`` in order until about budget_s; None where
+    that library is not built."""
     from oracle import Reference, ReferenceDescriptor
 
     if not Reference.available():
@@ -237,51 +365,47 @@ def reference_forward_rate(spec, cfg, budget_s=4.0, threads=None):
                                              spec["switch_flag"], spec["bzero_flag"], ns, cm, spec["weights"])
     else:
         ref = ReferenceDescriptor.symmetry_functions(ns, cm, spec["types"], spec["sizes"], spec["params"])
-
-    def run(n):
+    atoms, secs = 0, 0.0
+    for cfg in cfgs:
         t0 = time.perf_counter()
-        ref.compute(np.array([n], np.int32), cfg.species, cfg.nbl, cfg.counts[:n], cfg.coords, n_configs=1,
+        ref.compute(np.array([cfg.n_atoms], np.int32), cfg.species, cfg.nbl, cfg.counts, cfg.coords, n_configs=1,
                     config_ptr=np.array([0], np.int32), n_threads=threads)
-        return time.perf_counter() - t0
+        secs += time.perf_counter() - t0
+        atoms += cfg.n_atoms
+        if secs >= budget_s:
+            break
+    return atoms / secs if secs > 0 else None
 
-    n0 = min(cfg.n_atoms, max(threads, 16))
-    t0 = run(n0)
-    n1 = int(min(cfg.n_atoms, max(n0, n0 * budget_s / max(t0, 1e-6))))
-    return n1 / run(n1)
 
-
-def mix_cpu_rate(specs, requests, budget_s):
+def mix_cpu(specs, requests, budget_s):
     """CPU desc+VJP atoms/s of the request mix: each lane's rate on a sample
-    of its own requests, combined by the lanes' atom shares."""
+    of its own requests (oracle desc+VJP, and the reference's own C++
+    forward), combined by the lanes' atom shares.  Returns (rate, sample
+    text, threads, reference forward rate, {rid: (desc, folded forces)} of
+    the requests sampled whole)."""
     threads = os.cpu_count() or 1
     atoms = {k: sum(r.n_atoms for r in requests if r.lane == k) for k in specs}
     tot = sum(atoms.values())
-    secs_per_atom, samples = 0.0, []
+    spa, spa_fwd, samples, outputs = 0.0, 0.0, [], {}
     for k, spec in specs.items():
-        cfgs = [r.cfg for r in requests if r.lane == k]
-        if not cfgs:
+        rs = [r for r in requests if r.lane == k]
+        if not rs:
             continue
-        r, n, _ = cpu_rate(spec, cfgs, budget_s=budget_s * atoms[k] / tot, threads=threads)
-        secs_per_atom += (atoms[k] / tot) / r
+        share = atoms[k] / tot
+        rate, n, _, whole = oracle_sample(spec, rs, budget_s=budget_s * share, threads=threads,
+                                          dEs=[r.dE for r in rs])
+        spa += share / rate
         samples.append(f"{n} {k} centres")
-    return 1.0 / secs_per_atom, ", ".join(samples), threads
+        for i, d, g in whole:
+            outputs[rs[i].rid] = (d, fold(g, rs[i].n_atoms, rs[i].image))
+        fwd = reference_forward_rate(spec, rs, budget_s=budget_s * share / 3, threads=threads)
+        spa_fwd = None if (fwd is None or spa_fwd is None) else spa_fwd + share / fwd
+    return 1.0 / spa, ", ".join(samples), threads, (1.0 / spa_fwd if spa_fwd else None), outputs
 
 
 # ------------------------------------------------------------------ serve
-def serve_setup(seed=1, n_pool=32):
-    from libdescriptor_b200 import serving as S
-
-    pool = S.packing_pool(n_pool, n_min=16, n_max=32768, seed=seed)
-    specs = {"sf": sf24_spec(["A", "B"]), "bs": bs_spec(8, ["A", "B"], [1.0, 0.5])}
-    return pool, specs
-
-
-def tag_requests(reqs, pool):
-    """Attach each request's pool configuration (for the resident pass)."""
-    by_id = {id(c.coords): c for c in pool}
-    for r in reqs:
-        r.cfg = by_id[id(r.coords)]
-    return reqs
+def serve_specs():
+    return {"sf": sf24_spec(["A", "B"]), "bs": bs_spec(8, ["A", "B"], [1.0, 0.5])}
 
 
 def run_serve(args, torch, lds, dev, world, rank, local, dist):
@@ -289,15 +413,17 @@ def run_serve(args, torch, lds, dev, world, rank, local, dist):
     from libdescriptor_b200 import flops as F
     from libdescriptor_b200 import serving as S
     from libdescriptor_b200 import workloads as W
+    from libdescriptor_b200.replicas import replica_throughput
 
-    pool, specs = serve_setup(seed=1 + rank)
+    specs = serve_specs()
     kinds = {k: make_descriptor(s) for k, s in specs.items()}
     widths = {k: int(v.width) for k, v in kinds.items()}
     K = args.steps
-    nreq = K * REQ_PER_STEP
-    reqs = tag_requests(S.make_requests(pool, nreq, widths, MIX, seed=11 + rank), pool)
-    # at most 10 distinct steps are kept resident; longer runs cycle over them
-    steps = [reqs[i * REQ_PER_STEP:(i + 1) * REQ_PER_STEP] for i in range(min(K, 10))]
+    t_gen = time.perf_counter()
+    reqs = S.request_stream(N_STREAM, widths, MIX, seed=11 + rank, device=dev)
+    gen_s = time.perf_counter() - t_gen
+    # the resident pass: K steps over (at most 10 distinct) groups of 200 requests
+    steps = [reqs[i * REQ_PER_STEP:(i + 1) * REQ_PER_STEP] for i in range(min(K, 10, N_STREAM // REQ_PER_STEP))]
 
     peak = lds.measure_fp64_peak(4096)
     weights = F.measure_weights(peak)
@@ -307,13 +433,12 @@ def run_serve(args, torch, lds, dev, world, rank, local, dist):
     for st in steps:
         per = {}
         for k in kinds:
-            cfgs = [r.cfg for r in st if r.lane == k]
-            if not cfgs:
+            rs = [r for r in st if r.lane == k]
+            if not rs:
                 continue
-            b = W.concat(cfgs)
-            db = B.DeviceBatch.from_batch(b, kinds[k], device=dev)
-            dE = torch.randn(db.n_rows, widths[k], dtype=torch.float64, device=dev)
-            per[k] = (B.BatchedPass(kinds[k], db, dE), sum(algorithmic_flops(specs[k], c, weights) for c in cfgs))
+            db = B.DeviceBatch.from_batch(W.concat(rs), kinds[k], device=dev)
+            dE = torch.as_tensor(np.concatenate([r.dE for r in rs]), device=dev)
+            per[k] = (B.BatchedPass(kinds[k], db, dE), sum(algorithmic_flops(specs[k], r, weights) for r in rs))
         passes.append(per)
     stream = torch.cuda.Stream(device=dev)
     for per in passes:
@@ -348,71 +473,95 @@ def run_serve(args, torch, lds, dev, world, rank, local, dist):
         ms = {k: sum(a.elapsed_time(b) for a, b in v) for k, v in evs.items()}
         step_atoms = [sum(r.n_atoms for r in st) for st in steps]
         atoms_timed = sum(step_atoms[i % len(steps)] for i in range(K))
-        atoms_total = sum(r.n_atoms for r in reqs)
         value, tot_ms, _ = replica_throughput(atoms_timed, sum(ms.values()), dist, dev)
         flops_timed = {k: sum(per[k][1] for i in range(K) for per in [passes[i % len(passes)]] if k in per)
                        for k in kinds}
+        bs_atoms_timed = sum(sum(r.n_atoms for r in steps[i % len(steps)] if r.lane == "bs") for i in range(K))
         del passes
         torch.cuda.empty_cache()
 
-        # ---- e2e: the server at every rate, and the plain per-call path
+        # ---- e2e: the server over the whole stream at every rate, then the
+        # plain per-call path on the same stream at every rate
         eng = S.ServingEngine(kinds, budget_bytes=40 << 30, shares={"sf": 0.45, "bs": 0.55}, device=dev)
-        warm = tag_requests(S.make_requests(pool, 64, widths, MIX, seed=99), pool)
-        eng.serve(warm, None)
-        sweep = []
-        h2d_bytes = sum(r.coords.nbytes + r.species.nbytes + r.image.nbytes + r.nbl.nbytes + r.counts.nbytes
-                        + r.dE.nbytes + 12 * r.n_atoms for r in reqs)
-        d2h_bytes = sum(8 * r.n_atoms * (widths[r.lane] + 3) for r in reqs)
-        served = None
+        eng.serve(reqs[:64], None)
+        kept = {}                       # results of the first step's requests, top rate
+
+        def keep_first_step(req):
+            if req.rid < REQ_PER_STEP:
+                kept[req.rid] = (np.array(req.desc), np.array(req.grad))
+
+        sweep, served, plain = [], {}, {}
         for rate in sorted(RATES):
-            rs = tag_requests(S.make_requests(pool, nreq, widths, MIX, seed=11 + rank), pool)
-            eng.sched.batch_rows, eng.sched.batch_reqs, eng.sched.n_batches = [], [], 0
+            sch = eng.sched
+            sch.batch_rows, sch.batch_reqs, sch.batch_lanes, sch.n_batches = [], [], [], 0
             eng.launches = 0
             t_b = time.time()
-            res = eng.serve(rs, S.poisson_arrivals(nreq, rate, seed=21))
+            res = eng.serve(reqs, S.poisson_arrivals(N_STREAM, rate, seed=21),
+                            on_done=keep_first_step if rate == max(RATES) else None)
             windows.append((t_b, time.time()))
-            res["rate_per_s"] = rate
-            sweep.append({k: (round(v, 4) if isinstance(v, float) else v) for k, v in res.items()})
-            served = res
+            served[rate] = res
         del eng
         torch.cuda.empty_cache()
-        rs = S.make_requests(pool, nreq, widths, MIX, seed=11 + rank)
-        plain = S.serve_plain(kinds, rs, S.poisson_arrivals(nreq, max(RATES), seed=21))
+        for rate in sorted(RATES):
+            plain[rate] = S.serve_plain(kinds, reqs, S.poisson_arrivals(N_STREAM, rate, seed=21))
+        for rate in sorted(RATES):
+            sv, pl = served[rate], plain[rate]
+            sweep.append({"rate_per_s": rate,
+                          "served": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in sv.items()},
+                          "plain": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in pl.items()},
+                          "served_over_plain": sv["atoms_per_s"] / pl["atoms_per_s"]})
     if rank != 0:
         return None
-    bs_flops, sf_flops = flops_timed["bs"], flops_timed["sf"]
-    bs_atoms_timed = sum(sum(r.n_atoms for r in steps[i % len(steps)] if r.lane == "bs") for i in range(K))
-    ach_bs = bs_flops / (ms["bs"] * 1e-3) / 1e12 if ms.get("bs") else 0.0
-    ach_sf = sf_flops / (ms["sf"] * 1e-3) / 1e12 if ms.get("sf") else 0.0
+    top = max(RATES)
+    ach_bs = flops_timed["bs"] / (ms["bs"] * 1e-3) / 1e12 if ms.get("bs") else 0.0
+    ach_sf = flops_timed["sf"] / (ms["sf"] * 1e-3) / 1e12 if ms.get("sf") else 0.0
     roof = {"bound": "fp64", "achieved": ach_bs, "peak": peak, "unit": "TFLOP/s", "frac": ach_bs / peak,
             "traffic": DRAM_BYTES_PER_ATOM["bs8"] * bs_atoms_timed / K,
             "traffic_note": "bytes per step of the bispectrum lane, ncu DRAM bytes per atom of the 8192-atom "
                             "launch (profiles/) times the lane's atoms per step",
             "kernel": BS_KERNELS + " (bispectrum 2J=8 lane of the batched pass)",
-            "flops_per_step": bs_flops / K, "share_of_pass_time": ms.get("bs", 0.0) / tot_ms,
+            "flops_per_step": flops_timed["bs"] / K, "share_of_pass_time": ms.get("bs", 0.0) / tot_ms,
+            "flop_count": "libdescriptor_b200/flops.py: U recursion + Z/B/Y + the reverse-mode pair sweep",
             "peak_source": "bench.py FP64 FMA probe (ld_measure_fp64_peak), same run; MEASURED_PEAKS.json has no "
                            "FP64 figure",
             "call_weights_flops": {k: round(v, 1) for k, v in weights.items()},
             "sf_lane": {"achieved": ach_sf, "frac": ach_sf / peak, "kernel": "sfg_kernel<1,1,0>",
                         "share_of_pass_time": ms.get("sf", 0.0) / tot_ms}}
-    cpu = None
+    cpu, parity = None, None
     if not args.no_cpu_baseline and world == 1:
-        r, sample, thr = mix_cpu_rate(specs, reqs[:REQ_PER_STEP], budget_s=12.0)
+        r, sample, thr, fwd, outs = mix_cpu(specs, reqs[:REQ_PER_STEP], budget_s=12.0)
         cpu = {"value": r, "unit": "atoms/s", "cores": thr, "kind": "port",
-               "sample": f"{sample} of the first step's requests (whole configurations in order), desc+VJP by "
-                         f"the oracle's analytic adjoint on all host threads, combined by the mix's atom shares"}
-    e2e = {"value": world * served["atoms_per_s"], "unit": "atoms/s",
-           "h2d_bytes_per_step": int(h2d_bytes / K), "d2h_bytes_per_step": int(d2h_bytes / K),
+               "sample": f"{sample} of the stream's first {REQ_PER_STEP} requests (whole requests in order), "
+                         f"desc+VJP by the oracle's analytic adjoint on all host threads, combined by the mix's "
+                         f"atom shares",
+               "reference_forward": {"value": fwd, "unit": "atoms/s", "kind": "reference",
+                                     "what": "the reference's own C++ forward (oracle/_ref) alone, same requests"}}
+        chk = Parity()
+        for rid, (d_ref, f_ref) in outs.items():
+            if rid in kept:
+                chk.add(f"served request {rid}", kept[rid][0], d_ref, kept[rid][1], f_ref)
+        parity = chk.summary("oracle desc + analytic VJP, served results at the top rate")
+    n_steps_stream = N_STREAM / REQ_PER_STEP
+    h2d_bytes = sum(r.coords.nbytes + r.species.nbytes + r.image.nbytes + r.nbl.nbytes + r.counts.nbytes
+                    + r.dE.nbytes + 12 * r.n_atoms for r in reqs)
+    d2h_bytes = sum(8 * r.n_atoms * (widths[r.lane] + 3) for r in reqs)
+    atoms_total = sum(r.n_atoms for r in reqs)
+    e2e = {"value": world * served[top]["atoms_per_s"], "unit": "atoms/s",
+           "h2d_bytes_per_step": int(h2d_bytes / n_steps_stream), "d2h_bytes_per_step": int(d2h_bytes / n_steps_stream),
            "api": "libdescriptor_b200.serving.ServingEngine.serve (host numpy requests in, host results out), "
-                  f"Poisson arrivals at {int(max(RATES))}/s",
-           "p50_ms": served["p50_ms"], "p99_ms": served["p99_ms"],
-           "plain_call": {"value": world * plain["atoms_per_s"], "p50_ms": plain["p50_ms"], "p99_ms": plain["p99_ms"],
+                  f"{N_STREAM} requests, Poisson arrivals at {int(top)}/s",
+           "p50_ms": served[top]["p50_ms"], "p99_ms": served[top]["p99_ms"],
+           "plain_call": {"value": world * plain[top]["atoms_per_s"], "p50_ms": plain[top]["p50_ms"],
+                          "p99_ms": plain[top]["p99_ms"],
                           "api": "libdescriptor_b200.compute_and_gradient per request + host fold"},
-           "served_over_plain": served["atoms_per_s"] / plain["atoms_per_s"],
+           "served_over_plain": served[top]["atoms_per_s"] / plain[top]["atoms_per_s"],
            "rate_sweep": sweep}
-    cdesc = {"workload": "served_mixed_stream_sf24_70_bs2J8_30", "requests": nreq, "requests_per_step": REQ_PER_STEP,
-             "atoms": int(atoms_total), "pool_configurations": len(pool), "atoms_log_uniform": [16, 32768],
+    cdesc = {"workload": "served_mixed_stream_sf24_70_bs2J8_30", "requests": N_STREAM,
+             "requests_per_step": REQ_PER_STEP, "atoms": int(atoms_total),
+             "atoms_per_request": "log-uniform in [16, 32768], drawn per request; each request its own periodic "
+                                  "packing cut from 4 random packings of 32768 atoms",
              "density": 0.05, "d_min": 2.0, "cutoff": 5.0, "mix": MIX, "hbm_budget_gb": 40,
+             "stream_setup_s": round(gen_s, 1),
              "l2": "inputs of every step (>= 100 MB per lane pass) exceed the 126 MB L2 footprint reuse; no flush",
              "value": "batched resident pass (one launch per lane per step, inputs in HBM)",
              "parallelism": f"replicas x{world}"}
@@ -420,8 +569,8 @@ def run_serve(args, torch, lds, dev, world, rank, local, dist):
         "metric": METRIC, "value": value, "unit": "atoms/s", "n_gpus": world, "steps": K, "warmup": args.warmup,
         "ms_per_step": tot_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded packings, no dataset)", "config": cdesc, "roofline": roof,
-        "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk.summary(windows),
-        "p50_ms": served["p50_ms"], "p99_ms": served["p99_ms"],
+        "cpu_baseline": cpu, "parity": parity, "e2e": e2e, "gpu_launches": int(launches),
+        "clocks": clk.summary(windows), "p50_ms": served[top]["p50_ms"], "p99_ms": served[top]["p99_ms"],
     }
 
 
@@ -433,19 +582,23 @@ def run_batch512(args, torch, lds, dev, world, rank, local, dist):
     from libdescriptor_b200 import tuner
     from libdescriptor_b200 import workloads as W
 
+    from libdescriptor_b200.replicas import replica_throughput
+
     cfgs = B.diamond_batch(512, seed=1 + rank)
     b = W.concat(cfgs)
     specs = {"sf24": sf24_spec(["Si"]), "bs6": bs_spec(6, ["Si"], [1.0])}
     kinds = {k: make_descriptor(s) for k, s in specs.items()}
     peak = lds.measure_fp64_peak(4096)
     weights = F.measure_weights(peak)
-    tu = tuner.Autotuner(cache_path=os.path.join(ROOT, "gpurun_out", "tuning_cache.json")
-                         if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else None)
-    passes, chosen, loop_ms = {}, {}, {}
+    # the launch-shape choices are cached per process (a fresh box each run)
+    tu = tuner.Autotuner(cache_path=None)
+    passes, chosen, loop_ms, dE_pass = {}, {}, {}, {}
     stream = torch.cuda.Stream(device=dev)
+    rng_p = np.random.default_rng(3 + rank)
     for k, kind in kinds.items():
         db = B.DeviceBatch.from_batch(b, kind, device=dev)
-        dE = torch.randn(db.n_rows, int(kind.width), dtype=torch.float64, device=dev)
+        dE_pass[k] = rng_p.normal(size=(db.n_rows, int(kind.width)))
+        dE = torch.as_tensor(dE_pass[k], device=dev)
         ps = B.BatchedPass(kind, db, dE, stream=stream)
         chosen[k] = tu.tune(ps, k, 0 if k.startswith("sf") else 1)
         # the per-configuration launch loop (same arena, one call per cell)
@@ -578,17 +731,30 @@ def run_batch512(args, torch, lds, dev, world, rank, local, dist):
             "kernel": f"{dom} batched pass", "flops_per_step": flop[dom],
             "share_of_step_time": ms[dom] / step_ms,
             "peak_source": "bench.py FP64 FMA probe (ld_measure_fp64_peak), same run"}
-    cpu = None
+    cpu, parity = None, None
     if not args.no_cpu_baseline and world == 1:
-        secs = 0.0
+        secs, secs_fwd = 0.0, 0.0
         samples = []
+        chk = Parity()
+        rp = passes[next(iter(passes))].db.row_ptr
         for k, spec in specs.items():
-            r, n, thr = cpu_rate(spec, cfgs, budget_s=6.0)
+            dEs = [dE_pass[k][rp[c]:rp[c + 1]] for c in range(len(cfgs))]
+            r, n, thr, whole = oracle_sample(spec, cfgs, budget_s=6.0, dEs=dEs)
             secs += 1.0 / r
+            fwd = reference_forward_rate(spec, cfgs, budget_s=2.0)
+            secs_fwd = None if (fwd is None or secs_fwd is None) else secs_fwd + 1.0 / fwd
             samples.append(f"{n} centres ({k})")
+            ps = passes[k]
+            for c, d, g in whole:
+                chk.add(f"batch512 {k} cell {c}", ps.descriptors(c).cpu().numpy(), d,
+                        ps.forces(c).cpu().numpy(), fold(g, cfgs[c].n_atoms, cfgs[c].image))
+        parity = chk.summary("oracle desc + analytic VJP, cells of the timed graph passes")
         cpu = {"value": 1.0 / secs, "unit": "atoms/s", "cores": os.cpu_count() or 1, "kind": "port",
                "sample": ", ".join(samples) + " of the cells in order; every atom gets both descriptors, desc+VJP "
-                                               "by the oracle on all host threads"}
+                                               "by the oracle on all host threads",
+               "reference_forward": {"value": (1.0 / secs_fwd) if secs_fwd else None, "unit": "atoms/s",
+                                     "kind": "reference",
+                                     "what": "the reference's own C++ forward (oracle/_ref), both descriptors"}}
     cdesc = {"workload": "batched_512_diamond_cells_sf24_and_bs2J6", "cells": 512, "atoms": int(n_rows),
              "n_cells_per_axis": "U{1..6}", "strain": 0.03, "jitter": 0.1, "cutoff": 5.0,
              "tuned_launch_shape": chosen,
@@ -600,7 +766,7 @@ def run_batch512(args, torch, lds, dev, world, rank, local, dist):
         "metric": METRIC, "value": value, "unit": "atoms/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded cells, no dataset)", "config": cdesc,
-        "roofline": roof, "cpu_baseline": cpu,
+        "roofline": roof, "cpu_baseline": cpu, "parity": parity,
         "e2e": {"value": world * n_rows / e2e_s, "unit": "atoms/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * e2e_s,
                 "api": "batch.DeviceBatch.from_batch once (pinned host batch) + BatchedPass.run per descriptor, "
@@ -616,6 +782,7 @@ def run_batch512(args, torch, lds, dev, world, rank, local, dist):
 # ----------------------------------------------------------- single cell
 def run_single(args, torch, lds, dev, world, rank, local, dist):
     from libdescriptor_b200 import flops as F
+    from libdescriptor_b200.replicas import replica_throughput
 
     cfg, spec, cdesc = make_workload(args.workload, seed=1 + rank)
     ds = make_descriptor(spec)
@@ -701,75 +868,90 @@ def run_single(args, torch, lds, dev, world, rank, local, dist):
             "call_weights_flops": {k: round(v, 1) for k, v in weights.items()},
             "hbm_bytes_per_step_algorithmic": int(cfg.coords.nbytes + cfg.nbl.nbytes + 8 * n * W * 2
                                                   + 24 * cfg.n_total)}
-    cpu = None
+    cpu, parity = None, None
     if not args.no_cpu_baseline and world == 1:
-        r, sample, thr = cpu_rate(spec, [cfg], budget_s=10.0)
-        fwd = reference_forward_rate(spec, cfg, budget_s=4.0)
+        r, sample, thr, whole = oracle_sample(spec, [cfg], budget_s=10.0, dEs=[dE_h])
+        fwd = reference_forward_rate(spec, [cfg], budget_s=4.0)
         cpu = {"value": r, "unit": "atoms/s", "cores": thr, "kind": "port",
-               "sample": f"{sample} of {n} centres, desc+VJP by the oracle's analytic adjoint on all host "
-                         f"threads; reference C++ forward alone: {None if fwd is None else round(fwd, 1)} atoms/s"}
+               "sample": f"{sample} of {n} centres, desc+VJP by the oracle's analytic adjoint on all host threads",
+               "reference_forward": {"value": fwd, "unit": "atoms/s", "kind": "reference",
+                                     "what": "the reference's own C++ forward (oracle/_ref) alone, same cell"}}
+        chk = Parity()
+        for _, d, g in whole:
+            chk.add(args.workload, desc.cpu().numpy(), d, dc.cpu().numpy(), g)
+        parity = chk.summary("oracle desc + analytic VJP, the last timed pass")
     return {
         "metric": METRIC, "value": value, "unit": "atoms/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, no dataset)",
         "config": dict(cdesc, l2="flushed between steps (256 MB write outside the timed events)",
                        parallelism=f"replicas x{world}"),
-        "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+        "roofline": roof, "cpu_baseline": cpu, "parity": parity, "e2e": e2e, "gpu_launches": int(launches),
         "clocks": clk.summary([(t_begin, t_end)]),
     }
 
 
 # -------------------------------------------------------- reference arm
 def run_reference(args):
-    """The reference-side CPU path of the same workload: the oracle's
-    desc+VJP (a restatement of the reference's algorithm; its Enzyme
-    gradient cannot be built offline) on all host threads."""
+    """The reference-side CPU path of the same workload on all host threads:
+    desc+VJP by the oracle's analytic adjoint (a restatement of the
+    reference's algorithm; its Enzyme gradient cannot be built offline), the
+    reference's own C++ forward (oracle/_ref) timed beside it.  Inputs come
+    from the same generators (synth.py by file path) with the reference's
+    own neighbour-list builder: nothing of this library is loaded."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    rates, sample = [], None
+    rates, fwd_rates, sample = [], [], None
     if args.workload == "serve":
-        from libdescriptor_b200 import serving as S
-
-        pool, specs = serve_setup(seed=1)
+        sy = _synth()
+        specs = serve_specs()
         widths = {"sf": 24, "bs": 55}
-        reqs = tag_requests(S.make_requests(pool, REQ_PER_STEP, widths, MIX, seed=11), pool)
+        reqs = []
+        for i, lane, cfg, dE in sy.stream_requests(N_STREAM, widths, MIX, ref_prepare, seed=11, last=REQ_PER_STEP):
+            cfg.rid, cfg.lane, cfg.dE = i, lane, dE
+            reqs.append(cfg)
 
         def one(budget):
-            return mix_cpu_rate(specs, reqs, budget)
+            r, smp, thr, fwd, _ = mix_cpu(specs, reqs, budget)
+            return r, smp, fwd
 
-        cdesc = {"workload": "served_mixed_stream_sf24_70_bs2J8_30", "requests_per_step": REQ_PER_STEP,
-                 "mix": MIX, "atoms_log_uniform": [16, 32768]}
+        cdesc = {"workload": "served_mixed_stream_sf24_70_bs2J8_30", "requests": N_STREAM,
+                 "requests_per_step": REQ_PER_STEP, "mix": MIX, "atoms_log_uniform": [16, 32768],
+                 "sampled": f"the stream's first {REQ_PER_STEP} requests"}
     elif args.workload == "batch512":
-        from libdescriptor_b200 import batch as B
-
-        cfgs = B.diamond_batch(512, seed=1)
+        cfgs = diamond_cells(512, seed=1, prepare=ref_prepare)
         specs = {"sf24": sf24_spec(["Si"]), "bs6": bs_spec(6, ["Si"], [1.0])}
 
         def one(budget):
-            secs, s = 0.0, []
+            secs, secs_fwd, smp = 0.0, 0.0, []
             for k, spec in specs.items():
-                r, n, _ = cpu_rate(spec, cfgs, budget_s=budget / 2)
+                r, n, _, _ = oracle_sample(spec, cfgs, budget_s=budget / 2)
                 secs += 1.0 / r
-                s.append(f"{n} centres ({k})")
-            return 1.0 / secs, ", ".join(s), threads
+                fwd = reference_forward_rate(spec, cfgs, budget_s=budget / 6)
+                secs_fwd = None if (fwd is None or secs_fwd is None) else secs_fwd + 1.0 / fwd
+                smp.append(f"{n} centres ({k})")
+            return 1.0 / secs, ", ".join(smp), (1.0 / secs_fwd if secs_fwd else None)
 
         cdesc = {"workload": "batched_512_diamond_cells_sf24_and_bs2J6", "cells": 512}
     else:
-        cfg, spec, cdesc = make_workload(args.workload, seed=1)
+        cfg, spec, cdesc = make_workload(args.workload, seed=1, prepare=ref_prepare)
 
         def one(budget):
-            return cpu_rate(spec, [cfg], budget_s=budget)
+            r, n, _, _ = oracle_sample(spec, [cfg], budget_s=budget)
+            return r, f"{n} of {cfg.n_atoms} centres", reference_forward_rate(spec, [cfg], budget_s=budget / 3)
 
     for _ in range(args.warmup):
         one(1.0)
     walls = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        r, sample, _ = one(6.0)
+        r, sample, fwd = one(6.0)
         walls.append(time.perf_counter() - t0)
         rates.append(r)
+        if fwd is not None:
+            fwd_rates.append(fwd)
     value = statistics.mean(rates)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "atoms/s", "n_gpus": args.gpus,
@@ -778,7 +960,11 @@ def run_reference(args):
         "data": "synthetic", "config": cdesc,
         "cpu_baseline": {"value": value, "unit": "atoms/s", "cores": threads, "kind": "port",
                          "sample": f"per step about 6 s of desc+VJP work: {sample}, by the oracle's analytic "
-                                   f"adjoint (the reference's Enzyme gradient cannot be built offline)"},
+                                   f"adjoint (the reference's Enzyme gradient cannot be built offline)",
+                         "reference_forward": {"value": statistics.mean(fwd_rates) if fwd_rates else None,
+                                               "unit": "atoms/s", "kind": "reference",
+                                               "what": "the reference's own C++ forward (oracle/_ref) alone, "
+                                                       "same inputs"}},
         "e2e": {"value": value, "unit": "atoms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

@@ -6,15 +6,22 @@ W_op flops, W_op measured on the device (``ld_measure_fp64_op_cost``: the
 FP64-pipe flops that fit in the time of one call).  Work is counted for the
 needed outputs only, along the loops of the kernels:
 
-bispectrum (twojmax J), per in-cutoff neighbour and per computed left-half
-element (j, ma, mb <= j/2; mirror rows of the middle column excluded):
-  U recursion       b-term 8 (ma >= 1) + a-term 10 (ma < j), Utot += 4
-  dU recursion      per direction: b-term 16, a-term 18
-  contraction       20 (S and three V sums)
-per Z element: 10 per (ma1, mb1) term + 4 per ma1 row; B: 4 per element;
-betaj: 2 per map entry; Y: 4 per (element, triple).
-Per neighbour calls: forward sqrt x3, tan, divide x2, cos; gradient adds
-sincos, tan, sqrt x2, divide x3, sin/cos of the switching function.
+bispectrum (twojmax J), along the three kernels of a descriptor + VJP pass:
+  U (one centre per CTA): per in-cutoff neighbour and computed left-half
+    element (j, ma, mb <= j/2; the middle column's mirrored rows excluded)
+    recursion b-term 8 (ma >= 1) + a-term 10 (ma < j), Utot += 4;
+    calls: sqrt x2, tan, divide x2, cos (switching function)
+  Z / B / Y (rows in lanes): per Z term 10 per (ma1, mb1) + 4 per ma1 row,
+    for the triples the outputs (forward) or the adjoint (gradient) need;
+    B 4 per element; betaj 2 per map entry; Y 4 per (element, triple)
+  pair gradient (reverse mode, one (centre, neighbour) pair per slot):
+    forward recompute of the recursion, 8 / 10 per element as above; the
+    backward sweep per element: seed 7 (ubar += w Y, S += w Re(conj(Y) u)),
+    then 20 per b-term and 20 per a-term (ubar of the two inputs, abar or
+    bbar), 2 per mirrored middle-column row and per element of a born
+    column (the copies reversed); per pair 24 (chain to x, y, z) + 15
+    (forces) + 4 per column (column sums); calls: sqrt x2, tan, divide x5,
+    sincos x2 (theta0, switching function)
 
 symmetry functions, per listed neighbour: staging 8 + sqrt + divide + cos;
 per pair output 6 + exp (g2); per triplet 25 + 2 sqrt + 3 divide + 2 cos
@@ -37,6 +44,13 @@ def measure_weights(fp64_tflops: float, iters: int = 2048) -> dict:
 
 DEFAULT_WEIGHTS = {"exp": 20.0, "sincos": 40.0, "sqrt": 12.0, "div": 12.0, "tan": 40.0,
                    "pow": 60.0, "cos": 30.0}
+
+
+# per-element and per-pair FP64 flops of the bispectrum kernels' loop bodies
+U_B, U_A, U_ACC = 8, 10, 4            # recursion b-term, a-term; Utot accumulation
+R_SEED, R_B, R_A, R_COPY = 7, 20, 20, 2
+R_PAIR, R_COL = 24 + 15, 4
+Z_TERM, Z_ROW, B_EL, BETA_ENTRY, Y_EL = 10, 4, 4, 2, 4
 
 
 @lru_cache(maxsize=None)
@@ -97,19 +111,38 @@ def _bs_tables(J: int, style: int):
     return elems, zf, zv, b_elems, len(outs), mentries, y_terms, len(trip_all)
 
 
+@lru_cache(maxsize=None)
+def bs_pair_reverse_flops(J: int) -> int:
+    """Flops of the reverse-mode pair kernel for one (centre, neighbour) pair,
+    without its library calls: forward recompute and backward sweep over the
+    left-half elements a lane column holds (the middle column's mirrored rows
+    excluded), the reversed copies, and the per-pair chain to the forces."""
+    f = 0
+    for j in range(1, J + 1):
+        h = j // 2
+        for mb in range(h + 1):
+            for ma in range(j + 1):
+                if j % 2 == 0 and mb == h and ma > h:
+                    f += R_COPY          # adjoint of the mirrored row
+                    continue
+                f += (U_B if ma >= 1 else 0) + (U_A if ma < j else 0)
+                f += R_SEED + (R_B if ma >= 1 else 0) + (R_A if ma < j else 0)
+        if j % 2 == 0 and j >= 2:
+            f += R_COPY * j              # the born column's inputs, reversed
+    return f + R_PAIR + R_COL * (J // 2 + 1)
+
+
 def bs_flops_per_atom(J: int, style: int, n_in: float, vjp: bool, w: dict | None = None) -> float:
+    """Algorithmic flops per centre with n_in in-cutoff neighbours."""
     w = w or DEFAULT_WEIGHTS
     elems, zf, zv, b_elems, nout, mentries, y_terms, _ = _bs_tables(J, style)
-    u_el = sum((8 if b else 0) + (10 if a else 0) + 4 for b, a in elems)
-    per_nb_fwd = u_el + 3 * w["sqrt"] + w["tan"] + 2 * w["div"] + w["cos"] + 20
+    u_el = sum((U_B if b else 0) + (U_A if a else 0) + U_ACC for b, a in elems)
+    per_nb_fwd = u_el + 2 * w["sqrt"] + w["tan"] + 2 * w["div"] + w["cos"]
     terms, rows, _ = zv if vjp else zf
-    z = 10 * terms + 4 * rows
-    f = n_in * per_nb_fwd + z + 4 * b_elems
+    f = n_in * per_nb_fwd + Z_TERM * terms + Z_ROW * rows + B_EL * b_elems
     if vjp:
-        du_el = sum(3 * ((16 if b else 0) + (18 if a else 0)) + 20 + (8 if b else 0) + (10 if a else 0)
-                    for b, a in elems)
-        per_nb_bwd = du_el + w["sincos"] + w["tan"] + 2 * w["sqrt"] + 3 * w["div"] + w["sincos"] + 40
-        f += n_in * per_nb_bwd + 2 * mentries + 4 * y_terms
+        per_pair = bs_pair_reverse_flops(J) + 2 * w["sqrt"] + w["tan"] + 5 * w["div"] + 2 * w["sincos"]
+        f += n_in * per_pair + BETA_ENTRY * mentries + Y_EL * y_terms
     return float(f)
 
 

@@ -15,72 +15,9 @@ import numpy as np
 
 from . import _libdescriptor as _ext
 
-# 8-atom conventional diamond basis (fractional)
-_DIAMOND = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0],
-                     [.25, .25, .25], [.25, .75, .75], [.75, .25, .75], [.75, .75, .25]])
-
-SF24_G2_ETA = (0.001, 0.005, 0.01, 0.02, 0.04, 0.08, 0.16, 0.32)
-SF24_G4_ETA = (0.001, 0.01, 0.03, 0.08)
-
-
-def sf24_params():
-    """The 24-d Behler set: 8 g2 (Rs = 0) + 16 g4 rows ordered (zeta, lambda, eta)."""
-    g2 = [[e, 0.0] for e in SF24_G2_ETA]
-    g4 = [[z, lam, e] for z in (1.0, 4.0) for lam in (-1.0, 1.0) for e in SF24_G4_ETA]
-    params = [v for row in g2 for v in row] + [v for row in g4 for v in row]
-    return ["g2", "g4"], [8, 2, 16, 3], params
-
-
-def diamond_cell(n1, n2, n3, a=5.43, jitter=0.0, strain=0.0, seed=0):
-    """Si diamond supercell of n1 x n2 x n3 conventional cells.  strain: each
-    cell-matrix entry perturbed by U(-strain, strain) (H = (I + eps) H0)."""
-    rng = np.random.default_rng(seed)
-    h0 = np.diag([n1 * a, n2 * a, n3 * a]).astype(np.float64)
-    eps = rng.uniform(-strain, strain, (3, 3)) if strain else np.zeros((3, 3))
-    cell = h0 @ (np.eye(3) + eps).T  # rows are lattice vectors
-    grid = np.array([[i, j, k] for i in range(n1) for j in range(n2) for k in range(n3)], dtype=np.float64)
-    frac = (grid[:, None, :] + _DIAMOND[None, :, :]).reshape(-1, 3) / np.array([n1, n2, n3])
-    x = frac @ cell
-    if jitter:
-        x = x + rng.normal(0.0, jitter, x.shape)
-    return np.ascontiguousarray(x), np.ascontiguousarray(cell)
-
-
-def random_packing(n, density=0.05, dmin=2.0, n_species=2, seed=0, max_tries=200):
-    """n atoms uniformly in a periodic cube of side (n/density)^(1/3) with a
-    minimum pair distance dmin (random sequential addition by rejection).
-    Species alternate 0,1,... so the mix is 50/50 for two species."""
-    from scipy.spatial import cKDTree
-
-    rng = np.random.default_rng(seed)
-    side = (n / density) ** (1.0 / 3.0)
-    acc = np.zeros((0, 3))
-    tries = 0
-    while acc.shape[0] < n:
-        tries += 1
-        if tries > max_tries:
-            raise RuntimeError("random_packing: could not place all atoms")
-        m = max(64, int(1.3 * (n - acc.shape[0])))
-        cand = rng.uniform(0.0, side, (m, 3))
-        if acc.shape[0]:
-            tree = cKDTree(acc, boxsize=side)
-            d, _ = tree.query(cand, k=1)
-            cand = cand[d >= dmin]
-        if cand.shape[0] == 0:
-            continue
-        ct = cKDTree(cand, boxsize=side)
-        pairs = ct.query_pairs(dmin, output_type="ndarray")
-        keep = np.ones(cand.shape[0], dtype=bool)
-        if pairs.size:
-            # greedy in index order: drop the later member of each close pair
-            order = np.argsort(pairs[:, 0], kind="stable")
-            for a, b in pairs[order]:
-                if keep[a] and keep[b]:
-                    keep[b] = False
-        cand = cand[keep][: n - acc.shape[0]]
-        acc = np.concatenate([acc, cand])
-    species = (np.arange(n) % n_species).astype(np.int32)
-    return np.ascontiguousarray(acc), np.eye(3) * side, species
+# the pure-numpy generators live in synth.py (importable without the extension)
+from .synth import (DIAMOND, SF24_G2_ETA, SF24_G4_ETA, diamond_cell,  # noqa: E402,F401
+                    random_packing, sf24_params)
 
 
 @dataclass
@@ -191,6 +128,12 @@ class DeviceConfig:
     @property
     def n_total(self) -> int:
         return int(self.coords.shape[0])
+
+    def to_host(self, cell=None) -> Config:
+        """The same configuration as host arrays (the ``prepare`` layout)."""
+        return Config(self.n_atoms, self.coords.cpu().numpy(), self.species.cpu().numpy(),
+                      self.image.cpu().numpy(), self.counts.cpu().numpy(), self.nbl.cpu().numpy(),
+                      None if cell is None else np.asarray(cell))
 
 
 def prepare_dev(coords, cell, species, cutoff, pbc=(1, 1, 1), device="cuda", stream=None) -> DeviceConfig:

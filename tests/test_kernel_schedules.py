@@ -178,3 +178,49 @@ def test_u_only_writer_fills_full_u_once(J):
     ref = np.concatenate([(U[j] + wself * np.eye(j + 1)).ravel() for j in range(J + 1)])
     assert (count == 1).all()
     np.testing.assert_allclose(out, ref, rtol=0, atol=1e-14)
+
+
+# ----------------------------------------------- roofline flop count
+W_MEASURED = {"exp": 41.2, "sincos": 89.2, "sqrt": 30.8, "div": 35.0, "tan": 89.9, "pow": 279.3, "cos": 74.9}
+
+
+@pytest.mark.parametrize("J", [2, 4, 6, 8])
+def test_pair_kernel_flop_count_walks_its_loops(J):
+    """The reverse-mode pair kernel (bsR_kernel): lane column mb runs layers
+    max(1, 2 mb) .. J forward (rev_fwd) and back (rev_bwd); per computed row
+    the recursion, the seed and the backward step; mirrored middle-column
+    rows only reverse their copy; at each even layer j the lane of column
+    j/2 - 1 takes back the j inputs it lent to the born column."""
+    from libdescriptor_b200 import flops as F
+
+    f = 0
+    for mb in range(J // 2 + 1):
+        for j in range(max(1, 2 * mb), J + 1):
+            h = j // 2
+            middle = j % 2 == 0 and mb == h
+            for ma in range(j + 1):
+                if middle and ma > h:
+                    f += F.R_COPY
+                    continue
+                b, a = ma >= 1, ma < j
+                f += F.U_B * b + F.U_A * a                    # forward recompute
+                f += F.R_SEED + F.R_B * b + F.R_A * a         # backward
+            if j % 2 == 0 and mb == h - 1:
+                f += F.R_COPY * j                             # birth of column h, reversed
+    f += F.R_PAIR + F.R_COL * (J // 2 + 1)
+    assert F.bs_pair_reverse_flops(J) == f
+
+
+def test_bispectrum_flops_per_atom_pinned():
+    """The per-atom count the benchmark's roofline divides by: 2J = 8,
+    style 3, 25 in-cutoff neighbours, descriptors + VJP, the call weights
+    measured on a B200 (FP64 flops in the time of one call)."""
+    from libdescriptor_b200 import flops as F
+
+    per_atom = F.bs_flops_per_atom(8, 3, 25.0, True, W_MEASURED)
+    assert abs(per_atom - 727777.5) < 1.0
+    # no forward-mode tangents: the gradient's per-neighbour work is the
+    # reverse sweep, under three times the forward recursion's 3.1 k flops
+    per_nb = F.bs_flops_per_atom(8, 3, 1.0, True, W_MEASURED) - F.bs_flops_per_atom(8, 3, 0.0, True, W_MEASURED)
+    fwd_nb = F.bs_flops_per_atom(8, 3, 1.0, False, W_MEASURED) - F.bs_flops_per_atom(8, 3, 0.0, False, W_MEASURED)
+    assert per_nb < 4 * fwd_nb
