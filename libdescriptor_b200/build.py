@@ -3,6 +3,8 @@
 Produces
   libdescriptor_b200/_lib/libldb200.so      C ABI (include/libdescriptor_b200.h):
                                              CUDA kernels + host core
+  libdescriptor_b200/_lib/libldb200_cxx.so  the reference's C++ driver API
+                                             (include/cxx/Descriptors.hpp) over it
   libdescriptor_b200/_libdescriptor*.so      pybind11 module over that ABI
 
 Run ``python libdescriptor_b200/build.py`` (or ``__graft_entry__.build()``); the
@@ -27,6 +29,7 @@ LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libldb200.so")
 EXT = sysconfig.get_config_var("EXT_SUFFIX") or ".so"
 MOD = os.path.join(HERE, "_libdescriptor" + EXT)
+CXX_LIB = os.path.join(LIBDIR, "libldb200_cxx.so")
 INCLUDE = os.path.join(ROOT, "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -81,11 +84,17 @@ def build(verbose: bool = False, jobs: int | None = None) -> None:
                 f.result()
     if _stale(LIB, objs):
         _run([nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lpthread", "-lgomp"], verbose)
+    # the C++ driver API (include/cxx/Descriptors.hpp) over the C ABI
+    cxx = shutil.which("g++") or "g++"
+    shim = os.path.join(CSRC, "ld_cxx.cpp")
+    shim_deps = [shim, LIB, os.path.join(INCLUDE, "cxx", "Descriptors.hpp"), os.path.join(CSRC, "ld_fd.h")] + HEADERS
+    if _stale(CXX_LIB, shim_deps):
+        _run([cxx, "-O2", "-std=c++17", "-shared", "-fPIC", "-I" + INCLUDE, shim, "-L" + LIBDIR, "-lldb200",
+              "-Wl,-rpath,$ORIGIN", "-o", CXX_LIB], verbose)
     pyb = os.path.join(CSRC, "ld_pybind.cpp")
-    if _stale(MOD, [pyb, LIB] + HEADERS):
+    if _stale(MOD, [pyb, LIB, os.path.join(CSRC, "ld_fd.h")] + HEADERS):
         import pybind11
 
-        cxx = shutil.which("g++") or "g++"
         py_inc = sysconfig.get_paths()["include"]
         _run([cxx, "-O2", "-std=c++17", "-shared", "-fPIC", "-fvisibility=hidden",
               "-I" + INCLUDE, "-I" + pybind11.get_include(), "-I" + py_inc, pyb,
