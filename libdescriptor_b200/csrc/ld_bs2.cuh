@@ -16,20 +16,20 @@
 // bsA_kernel<J, VJP, UOUT>  one CTA per centre: stage neighbours, U (column
 //                     lanes, slots reduced through a per-warp buffer), Z (LPT
 //                     task lists), B; for the gradient also Y = sum betaj Z ->
-//                     HBM.  UOUT (the split form's first kernel): U only,
-//                     written as full U blocks [row / 32][element][row % 32].
+//                     HBM.  UOUT (the split form's first kernel at 2J = 9):
+//                     U only, written as full U blocks [row / 32][element][row % 32].
 // bsZ_kernel<J, VJP, GSH>  split form: one CTA per 32 rows, a row per lane;
 //                     warp-uniform Z by rotating register windows over the
 //                     rows' U in shared memory, B, and Y = sum betaj Z -> HBM.
+// bsU_kernel<J>       split form's U for 2J <= 8: one warp per centre, slots of
+//                     column lanes over the neighbours, each column's sums over
+//                     all layers in registers, one slot reduction per centre.
 // bsR_kernel<J>       pair-parallel gradient, reverse mode: one slot per
 //                     (centre, neighbour) pair runs the column recursion
 //                     forward (layer inputs kept in shared memory) and then
 //                     carries dPhi/du backward to dPhi/da, dPhi/db; chained to
 //                     the position with the Cayley-Klein derivatives, FP64
 //                     atomics onto the neighbour and the centre.
-// bsB_kernel<J>       the forward-mode form of the same gradient (u and the
-//                     three du/dr tangents carried together); kept for
-//                     comparison, built with LD_BS_REVERSE=0.
 #pragma once
 
 #include "ld_internal.h"
