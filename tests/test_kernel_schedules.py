@@ -224,3 +224,48 @@ def test_bispectrum_flops_per_atom_pinned():
     per_nb = F.bs_flops_per_atom(8, 3, 1.0, True, W_MEASURED) - F.bs_flops_per_atom(8, 3, 0.0, True, W_MEASURED)
     fwd_nb = F.bs_flops_per_atom(8, 3, 1.0, False, W_MEASURED) - F.bs_flops_per_atom(8, 3, 0.0, False, W_MEASURED)
     assert per_nb < 4 * fwd_nb
+
+
+# ------------------------------------------- warp-per-centre U kernel
+def _lblock(j):
+    return sum((jj + 1) * (jj // 2 + 1) for jj in range(j))
+
+
+@pytest.mark.parametrize("J", [0, 1, 2, 3, 4, 5, 6, 7, 8])
+def test_warp_u_slot_reduction_covers_the_left_half(J):
+    """bsU_kernel: lane (slot, mb) puts its column's sums of every layer j >=
+    2 mb into the slot's row of the buffer at e = lblock(j) + ma (j/2+1) + mb,
+    the middle column's mirrored rows left out; over the lanes of one slot
+    every other left-half element is written exactly once, and the padded
+    per-slot stride (= NC mod 16 doubles) sends a half-warp's 16 lanes to 16
+    different banks for every (j, ma) they write together."""
+    NC = J // 2 + 1
+    SL = 32 // NC
+    nL = _lblock(J + 1)
+    RS = nL + ((NC - nL) % 16 + 16) % 16
+    assert RS >= nL and RS % 16 == NC % 16
+    seen = {}
+    for mb in range(NC):
+        for j in range(J + 1):
+            h = j // 2
+            if mb > h:
+                continue
+            for ma in range(j + 1):
+                if j % 2 == 0 and ma > h and mb == h:
+                    continue
+                e = _lblock(j) + ma * (h + 1) + mb
+                assert 0 <= e < nL
+                seen[e] = seen.get(e, 0) + 1
+    mirrors = sum(j // 2 for j in range(0, J + 1, 2))
+    assert len(seen) == nL - mirrors and all(v == 1 for v in seen.values())
+    for j in range(J + 1):
+        h = j // 2
+        for ma in range(j + 1):
+            for half in (0, 16):
+                banks = []
+                for lane in range(half, half + 16):
+                    slot, mb = divmod(lane, NC)
+                    if slot >= SL or mb > h or (j % 2 == 0 and ma > h and mb == h):
+                        continue
+                    banks.append((slot * RS + _lblock(j) + ma * (h + 1) + mb) % 16)
+                assert len(banks) == len(set(banks))
