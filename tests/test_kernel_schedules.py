@@ -269,3 +269,50 @@ def test_warp_u_slot_reduction_covers_the_left_half(J):
                         continue
                     banks.append((slot * RS + _lblock(j) + ma * (h + 1) + mb) % 16)
                 assert len(banks) == len(set(banks))
+
+
+# ------------------------------------------- pair kernel row search
+def _warp_search(off, n_rows, q0):
+    """bsR_kernel's 32-ary search, lane by lane."""
+    lo, hi = 0, n_rows - 1
+    rounds = 0
+    while hi > lo:
+        span = hi - lo
+        pos = [lo + (span * (lane + 1) + 31) // 32 for lane in range(32)]
+        le = [off[p] <= q0 for p in pos]
+        assert all(le[i] >= le[i + 1] for i in range(31)), "ballot not a prefix"
+        k = max((i for i in range(32) if le[i]), default=-1)
+        nlo = pos[k] if k >= 0 else lo
+        nhi = pos[k + 1] - 1 if k < 31 else hi
+        assert nlo <= nhi
+        lo, hi = nlo, nhi
+        rounds += 1
+    return lo, rounds
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_pair_kernel_row_search_finds_the_last_row_at_or_below(seed):
+    """The warp's first pair q0 lies in row r with off[r] <= q0 < off[r+1]
+    (rows without neighbours share their offset with the next row: the last
+    such row is the one that holds the pair); each slot then steps forward."""
+    rng = np.random.default_rng(seed)
+    n_rows = int(rng.integers(1, 40000))
+    counts = rng.integers(0, 40, n_rows)
+    counts[rng.random(n_rows) < 0.1] = 0
+    off = np.concatenate([[0], np.cumsum(counts)])
+    n_pairs = int(off[-1])
+    if n_pairs == 0:
+        return
+    for q0 in list(rng.integers(0, n_pairs, 200)) + [0, n_pairs - 1]:
+        row, rounds = _warp_search(off, n_rows, int(q0))
+        want = int(np.searchsorted(off, q0, side="right")) - 1
+        assert row == want and off[row] <= q0 < off[row + 1]
+        assert rounds <= 4
+        for slot in range(6):
+            qp = int(q0) + slot
+            if qp >= n_pairs:
+                break
+            r = row
+            while r + 1 < n_rows and off[r + 1] <= qp:
+                r += 1
+            assert off[r] <= qp < off[r + 1]
