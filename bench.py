@@ -57,13 +57,13 @@ sys.path.insert(0, ROOT)
 METRIC = "desc+VJP atoms/s, 1 B200: served batch vs plain call; p50/p99 ms @≤1e-10 rel"
 # DRAM bytes (read + write) per centre atom of the dominant kernels, from one
 # ncu capture each (profiles/, cold caches): bispectrum 2J=8 pass (U kernel
-# bsA<8,0,1> 1.41 MB, Z kernel bsZ 41.50 MB -- of which the 37.4 MB U blocks
-# that the U kernel has just written, an L2 hit outside the profiler -- and
-# the pair gradient bsR 21.98 MB, 8192-atom launch) and the factored
-# symmetry-function kernel (4096-atom launch: 1.75 MB).  Traffic grows with
+# bsU 1.34 MB, Z kernel bsZ 41.50 MB -- of which the 37.4 MB U blocks that
+# the U kernel has just written, an L2 hit outside the profiler -- and the
+# pair gradient bsR 21.98 MB, 8192-atom launch) and the factored
+# symmetry-function kernel (4096-atom launch: 1.73 MB).  Traffic grows with
 # the centres processed, so other launch sizes are scaled by their atom counts.
-DRAM_BYTES_PER_ATOM = {"bs8": (1.414656e6 + 41.50528e6 + 21.975296e6) / 8192, "sf24": 1.747968e6 / 4096}
-BS_KERNELS = "bsA_kernel<8,0,1> (U) + bsZ_kernel<8,1,1> (Z, B, Y) + bsR_kernel<8> (pair gradient)"
+DRAM_BYTES_PER_ATOM = {"bs8": (1.344512e6 + 41.504768e6 + 21.98016e6) / 8192, "sf24": 1.731328e6 / 4096}
+BS_KERNELS = "bsU_kernel<8> (U) + bsZ_kernel<8,1,1> (Z, B, Y) + bsR_kernel<8> (pair gradient)"
 RATES = (1000.0, 10000.0, 50000.0)
 N_STREAM = 20000
 REQ_PER_STEP = 200
@@ -420,7 +420,8 @@ def run_serve(args, torch, lds, dev, world, rank, local, dist):
     widths = {k: int(v.width) for k, v in kinds.items()}
     K = args.steps
     t_gen = time.perf_counter()
-    reqs = S.request_stream(N_STREAM, widths, MIX, seed=11 + rank, device=dev)
+    reqs = S.request_stream(N_STREAM, widths, MIX, seed=11 + rank, device=dev,
+                            processes=max(1, min(16, (os.cpu_count() or 1) // max(world, 1))))
     gen_s = time.perf_counter() - t_gen
     # the resident pass: K steps over (at most 10 distinct) groups of 200 requests
     steps = [reqs[i * REQ_PER_STEP:(i + 1) * REQ_PER_STEP] for i in range(min(K, 10, N_STREAM // REQ_PER_STEP))]

@@ -648,12 +648,14 @@ def packing_pool(n_pool: int, n_min: int = 16, n_max: int = 32768, density: floa
 
 def request_stream(n_req: int, widths: dict, mix: dict, n_min: int = 16, n_max: int = 32768,
                    density: float = 0.05, dmin: float = 2.0, cutoff: float = 5.0, seed: int = 0,
-                   source=None, grads=None, first: int = 0, last: int | None = None, device=None) -> list:
+                   source=None, grads=None, first: int = 0, last: int | None = None, device=None,
+                   processes: int = 1) -> list:
     """Requests first .. last-1 of the served stream (``synth.stream_requests``):
     per request its own log-uniform atom count, lane and periodic two-species
     packing, ghosts and neighbour lists built on the device when one is given
     (``workloads.prepare_dev``, identical to the host builder's lists) else on
-    the host, and a run of N(0, 1) dL/d(desc) rows."""
+    the host, and a run of N(0, 1) dL/d(desc) rows.  ``processes`` > 1 cuts
+    the packings in that many spawned worker processes."""
     from . import synth
     from . import workloads as Wk
 
@@ -664,7 +666,7 @@ def request_stream(n_req: int, widths: dict, mix: dict, n_min: int = 16, n_max: 
         prep = Wk.prepare
     reqs = []
     for i, lane, cfg, dE in synth.stream_requests(n_req, widths, mix, prep, n_min, n_max, density, dmin, cutoff,
-                                                  seed, source, grads, first, last):
+                                                  seed, source, grads, first, last, processes):
         r = Request(i, lane, cfg.n_atoms, cfg.coords, cfg.species, cfg.image, cfg.counts, cfg.nbl, dE)
         r.cfg = cfg
         reqs.append(r)

@@ -93,40 +93,85 @@ def random_packing(n, density=0.05, dmin=2.0, n_species=2, seed=0, max_tries=200
 class PackingSource:
     """Periodic random packings of any size cut out of a few large ones."""
 
-    def __init__(self, n_base=4, base_atoms=32768, density=0.05, dmin=2.0, seed=0):
+    def __init__(self, n_base=4, base_atoms=32768, density=0.05, dmin=2.0, seed=0, bases=None):
+        from scipy.spatial import cKDTree
+
         self.density, self.dmin = float(density), float(dmin)
-        self.bases = [random_packing(base_atoms, density, dmin, n_species=1, seed=seed * 1000 + 17 + i)[0]
-                      for i in range(n_base)]
+        self.bases = bases if bases is not None else [
+            random_packing(base_atoms, density, dmin, n_species=1, seed=seed * 1000 + 17 + i)[0]
+            for i in range(n_base)]
         self.side = (base_atoms / density) ** (1.0 / 3.0)
+        # periodic trees of the bases: a small cube is gathered from the ball
+        # around its centre instead of a scan of the whole base
+        self.trees = [cKDTree(np.clip(b, 0.0, np.nextafter(self.side, 0.0)), boxsize=self.side)
+                      for b in self.bases]
+
+    def _candidates(self, b, o, L):
+        """Indices of base b's atoms that may lie in the cube [o, o + L) (periodic)."""
+        if L > 0.45 * self.side:
+            return None
+        c = np.mod(o + 0.5 * L, self.side)
+        return np.asarray(self.trees[b].query_ball_point(c, 0.5 * np.sqrt(3.0) * L * (1.0 + 1e-9)), dtype=np.int64)
 
     def cut(self, n, rng, n_species=2):
         """About n atoms in a periodic cube of side (n / density)^(1/3):
         coordinates, cell (rows = lattice vectors), species (alternating)."""
-        from scipy.spatial import cKDTree
-
         L = min((n / self.density) ** (1.0 / 3.0), self.side)
         for _ in range(100):
-            base = self.bases[int(rng.integers(len(self.bases)))]
-            x = np.mod(base - rng.uniform(0.0, self.side, 3), self.side)
+            b = int(rng.integers(len(self.bases)))
+            o = rng.uniform(0.0, self.side, 3)
+            cand = self._candidates(b, o, L)
+            x = (self.bases[b] if cand is None else self.bases[b][np.sort(cand)]) - o
+            x += (x < 0.0) * self.side
+            x[x >= self.side] -= self.side
             if L < self.side:
-                x = x[np.all(x < L, axis=1)]
+                x = x[(x[:, 0] < L) & (x[:, 1] < L) & (x[:, 2] < L)]
             if x.shape[0] < 2:
                 continue
-            near = np.nonzero(np.any((x < self.dmin) | (x > L - self.dmin), axis=1))[0]
-            keep = np.ones(x.shape[0], dtype=bool)
-            if near.size > 1:
-                # only pairs that meet through the new periodic faces can be
-                # closer than dmin (the base packing keeps every other pair apart)
-                xs = np.clip(x[near], 0.0, np.nextafter(L, 0.0))
-                pairs = cKDTree(xs, boxsize=L).query_pairs(self.dmin, output_type="ndarray")
-                sub = _drop_close_pairs(pairs, np.ones(near.size, dtype=bool))
-                keep[near[~sub]] = False
-            x = x[keep]
-            x[x >= L] -= L          # np.mod may round up to the side itself
+            x = x[_face_conflicts_kept(x, L, self.dmin)]
             x = np.ascontiguousarray(x)
             if x.shape[0] >= 2:
                 return x, np.eye(3) * L, (np.arange(x.shape[0]) % n_species).astype(np.int32)
         raise RuntimeError("PackingSource.cut: no configuration with two atoms")
+
+
+def _face_conflicts_kept(x, L, dmin):
+    """Mask of the atoms kept when the cube [0, L)^3 is made periodic: only
+    atoms within dmin of a face can meet another one closer than dmin
+    through the new periodic faces (every other pair is at least dmin apart
+    already).  Those pairs are found among the near-face atoms and their
+    images shifted by -L along the axes where they lie near the upper face;
+    the later atom of each close pair is dropped."""
+    from scipy.spatial import cKDTree
+
+    keep = np.ones(x.shape[0], dtype=bool)
+    hi = x > L - dmin
+    near = np.nonzero((x < dmin).any(axis=1) | hi.any(axis=1))[0]
+    if near.size < 2:
+        return keep
+    pts, owner = [x[near]], [near]
+    hn = hi[near]
+    for mask in range(1, 8):
+        axes = [d for d in range(3) if mask >> d & 1]
+        sel = np.all(hn[:, axes], axis=1)
+        if sel.any():
+            sh = x[near[sel]].copy()
+            sh[:, axes] -= L
+            pts.append(sh)
+            owner.append(near[sel])
+    pts = np.concatenate(pts)
+    owner = np.concatenate(owner)
+    pairs = cKDTree(pts).query_pairs(dmin, output_type="ndarray")
+    if pairs.size == 0:
+        return keep
+    a, b = owner[pairs[:, 0]], owner[pairs[:, 1]]
+    m = a != b
+    if not m.any():
+        return keep
+    # the later atom of every close pair goes (a superset of a greedy pass:
+    # every remaining pair is at least dmin apart)
+    keep[np.maximum(a[m], b[m])] = False
+    return keep
 
 
 def stream_draws(n_req, mix, n_min=16, n_max=32768, seed=0):
@@ -155,19 +200,59 @@ class GradientPool:
         return self.blocks[lane][o:o + rows]
 
 
+_WORKER_SOURCE = None
+
+
+def _cut_worker_init(bases, base_atoms, density, dmin):
+    global _WORKER_SOURCE
+    _WORKER_SOURCE = PackingSource(base_atoms=base_atoms, density=density, dmin=dmin, bases=bases)
+
+
+def _cut_chunk(args):
+    seed, first, sizes = args
+    out = []
+    for k, n in enumerate(sizes):
+        x, cell, _ = _WORKER_SOURCE.cut(int(n), np.random.default_rng([seed, first + k]))
+        out.append((x, float(cell[0, 0])))
+    return out
+
+
+def stream_cuts(n_req, mix, n_min=16, n_max=32768, seed=0, source=None, first=0, last=None, processes=1):
+    """The packings (coordinates, cube side) of requests first .. last-1,
+    computed in ``processes`` spawned worker processes when > 1 (the cuts
+    hold the interpreter lock; spawning is safe after CUDA is in use)."""
+    sizes, _ = stream_draws(n_req, mix, n_min, n_max, seed)
+    last = n_req if last is None else min(last, n_req)
+    source = source or PackingSource(seed=seed)
+    if processes <= 1 or last - first < 256:
+        return [(lambda x: (x[0], float(x[1][0, 0])))(source.cut(int(sizes[i]), np.random.default_rng([seed, i])))
+                for i in range(first, last)]
+    import multiprocessing as mp
+
+    chunk = max(64, (last - first) // (8 * processes))
+    jobs = [(seed, c, sizes[c:min(c + chunk, last)]) for c in range(first, last, chunk)]
+    base_atoms = int(round(source.density * source.side ** 3))
+    with mp.get_context("spawn").Pool(processes, initializer=_cut_worker_init,
+                                      initargs=(source.bases, base_atoms, source.density, source.dmin)) as pool:
+        parts = pool.map(_cut_chunk, jobs)
+    return [c for part in parts for c in part]
+
+
 def stream_requests(n_req, widths, mix, prepare, n_min=16, n_max=32768, density=0.05, dmin=2.0, cutoff=5.0,
-                    seed=0, source=None, grads=None, first=0, last=None):
+                    seed=0, source=None, grads=None, first=0, last=None, processes=1):
     """Requests first .. last-1 of an n_req-request stream as (i, lane, cfg,
     dE): request i's atom count and lane come from ``stream_draws``, its
     packing from ``source.cut`` with the generator seeded by (seed, i), its
     ghosts and neighbour lists from ``prepare(coords, cell, species,
-    cutoff)`` (any builder of the reference's layout), its dL/d(desc) from
-    ``grads``.  Request i depends only on (seed, i)."""
-    sizes, lanes = stream_draws(n_req, mix, n_min, n_max, seed)
+    cutoff)`` (any builder of the reference's layout), its dL/d(desc) rows
+    from ``grads`` at an offset drawn from (seed, i, 1).  Request i depends
+    only on (seed, i)."""
+    _, lanes = stream_draws(n_req, mix, n_min, n_max, seed)
+    last = n_req if last is None else min(last, n_req)
     source = source or PackingSource(density=density, dmin=dmin, seed=seed)
     grads = grads or GradientPool(widths, n_max, seed)
-    for i in range(first, n_req if last is None else min(last, n_req)):
-        rng = np.random.default_rng([seed, i])
-        x, cell, sp = source.cut(int(sizes[i]), rng)
-        cfg = prepare(x, cell, sp, cutoff)
-        yield i, lanes[i], cfg, grads.take(lanes[i], cfg.n_atoms, rng)
+    cuts = stream_cuts(n_req, mix, n_min, n_max, seed, source, first, last, processes)
+    for i, (x, L) in zip(range(first, last), cuts):
+        sp = (np.arange(x.shape[0]) % 2).astype(np.int32)
+        cfg = prepare(x, np.eye(3) * L, sp, cutoff)
+        yield i, lanes[i], cfg, grads.take(lanes[i], cfg.n_atoms, np.random.default_rng([seed, i, 1]))
