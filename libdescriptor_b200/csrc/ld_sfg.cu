@@ -30,6 +30,12 @@ constexpr int NA = kSFGA, NR = kSFGR;
 #define LD_SFG_MINB 4
 #endif
 constexpr int kGPExtra = (LD_SFG_GP_SHARED ? 2 * NA * NR : 0);
+// radial terms of a triplet: 0 binary powering per term, 1 shared squarings
+// and balanced products (exponents below 2^kSFGPowBits), 2 one exp per term
+#ifndef LD_SFG_RADIAL
+#define LD_SFG_RADIAL 0
+#endif
+constexpr int kSFGPowBits = 8;
 
 // Paths the usual parameter sets never take (non-integer zeta, an eta that
 // is not an integer multiple of its group's smallest, cosine radial terms)
@@ -260,6 +266,41 @@ sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue)
                         // radial terms: one exp, integer multiples of the
                         // smallest eta by binary powering
                         double E[NR];
+#if LD_SFG_RADIAL == 2
+                        // every radial term by its own exp (independent chains)
+#pragma unroll
+                        for (int y = 0; y < NR; ++y) E[y] = y < g.nr[ty] ? exp(-g.eta[ty][y] * Ssum) : 0.0;
+#elif LD_SFG_RADIAL == 1
+                        // the squarings E0^(2^k) once, then each power as a
+                        // balanced product of the squarings its exponent's
+                        // bits select (dependent chain: 7 squarings + 3)
+                        {
+                            double P[kSFGPowBits];
+                            P[0] = exp(-g.eta[ty][0] * Ssum);
+#pragma unroll
+                            for (int k = 1; k < kSFGPowBits; ++k) P[k] = P[k - 1] * P[k - 1];
+                            E[0] = g.nr[ty] > 0 ? P[0] : 0.0;
+#pragma unroll
+                            for (int y = 1; y < NR; ++y) {
+                                E[y] = 0.0;
+                                if (y < g.nr[ty]) {
+                                    const int ec = g.ec[ty][y];
+                                    if (ec >= 2 && ec < (1 << kSFGPowBits)) {
+                                        double m[kSFGPowBits];
+#pragma unroll
+                                        for (int k = 0; k < kSFGPowBits; ++k) m[k] = (ec >> k) & 1 ? P[k] : 1.0;
+#pragma unroll
+                                        for (int w = 1; w < kSFGPowBits; w *= 2)
+#pragma unroll
+                                            for (int k = 0; k + w < kSFGPowBits; k += 2 * w) m[k] *= m[k + w];
+                                        E[y] = m[0];
+                                    } else {
+                                        E[y] = exp_cold(-g.eta[ty][y] * Ssum);
+                                    }
+                                }
+                            }
+                        }
+#else
 #pragma unroll
                         for (int y = 0; y < NR; ++y) {
                             E[y] = 0.0;
@@ -277,6 +318,7 @@ sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue)
                                 }
                             }
                         }
+#endif
                         // angular terms
                         double cp[NA], dcp[NA];
 #pragma unroll
