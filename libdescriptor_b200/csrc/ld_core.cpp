@@ -858,6 +858,9 @@ static int validate(const ld_descriptor *d, const HostRows &h, int n_total, cons
 }
 
 int launch_rows(ld_descriptor *d, const RowArgs &a0, cudaStream_t s) {
+    NvtxRange range(d->kind == LD_KIND_SYMMETRY_FUNCTIONS
+                        ? (a0.dE ? "ld: symmetry functions desc+VJP" : "ld: symmetry functions desc")
+                        : (a0.dE ? "ld: bispectrum desc+VJP" : "ld: bispectrum desc"));
     RowArgs a = a0;
     a.sf_warps = d->tune[LD_TUNE_SF_WARPS];
     a.ctas_per_sm = d->tune[LD_TUNE_CTAS_PER_SM];
@@ -922,6 +925,7 @@ static int host_pass_impl(ld_descriptor *d, HostRows &h, int n_total, const int 
 static int host_pass(ld_descriptor *d, HostRows &h, int n_total, const int *species, const int *nbl,
                      const double *coords, const double *dE, double *dcoords, double *desc,
                      int jac_width = 0) {
+    NvtxRange range("ld: host-buffer call (stage, launch, read back)");
     try {
         return host_pass_impl(d, h, n_total, species, nbl, coords, dE, dcoords, desc, jac_width);
     } catch (const std::bad_alloc &) {

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cstdint>
 #include <string>
@@ -28,6 +29,15 @@ enum DeviceStatus : int {
     kDevOk = 0,
     kDevCapacity = 1,   // a row exceeded max_neigh
     kDevBadIndex = 2,   // neighbour / centre index outside coords
+};
+
+// NVTX range over a scope (header-only NVTX 3: inert unless a profiler such
+// as Nsight Systems or ncu's range filter is attached).
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
 };
 
 // Launch accounting (all kernels of the library).

@@ -463,6 +463,14 @@ class ServingEngine:
         """Pinned staging + rebased uploads of one admitted request
         (``ld_stage_request``, native)."""
         torch = self.torch
+        torch.cuda.nvtx.range_push(f"serve: stage request {req.rid}")
+        try:
+            self._stage(req)
+        finally:
+            torch.cuda.nvtx.range_pop()
+
+    def _stage(self, req: Request) -> None:
+        torch = self.torch
         ln = self.lanes[req.lane]
         r0, a0, e0 = req.slots
         n, nt, nnz, W = req.n_atoms, req.n_total, req.nnz, ln.W
@@ -490,6 +498,14 @@ class ServingEngine:
         self.host_stage_s += time.perf_counter() - t_in
 
     def launch(self, plan: BatchPlan) -> None:
+        torch = self.torch
+        torch.cuda.nvtx.range_push(f"serve: {plan.lane} batch of {plan.n_rows} rows")
+        try:
+            self._launch(plan)
+        finally:
+            torch.cuda.nvtx.range_pop()
+
+    def _launch(self, plan: BatchPlan) -> None:
         torch = self.torch
         ln = self.lanes[plan.lane]
         r0, n = plan.row0, plan.n_rows
