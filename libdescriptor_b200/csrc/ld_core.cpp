@@ -888,6 +888,7 @@ static int status_error(ld_descriptor *d, cudaStream_t s, int st) {
         LDB_CUDA(cudaMemsetAsync(d->status.p, 0, sizeof(int), s));
         LDB_CUDA(cudaStreamSynchronize(s));
         if (st == kDevCapacity) return fail(LD_ERR_CAPACITY, "a centre has more neighbours than max_neigh");
+        if (st == kDevTimeout) return fail(LD_ERR_TIMEOUT, "a kernel's bounded wait for its shared-memory tile ran out");
         return fail(LD_ERR_INVALID_ARG, "a neighbour or centre index lies outside the coordinates");
     }
     return LD_OK;

@@ -29,6 +29,7 @@ enum DeviceStatus : int {
     kDevOk = 0,
     kDevCapacity = 1,   // a row exceeded max_neigh
     kDevBadIndex = 2,   // neighbour / centre index outside coords
+    kDevTimeout = 3,    // a bounded wait on an asynchronous copy ran out
 };
 
 // NVTX range over a scope (header-only NVTX 3: inert unless a profiler such
