@@ -468,13 +468,54 @@ def run_serve(args, torch, lds, dev, world, rank, local, dist):
                     evs[k].append((e0, e1))
         torch.cuda.synchronize()
         windows.append((t_a, time.time()))
+        for ps, _ in passes[0].values():
+            ps.sync_status()
+        # per-lane kernel times (the roofline's denominators): lanes in turn
+        ms = {k: sum(a.elapsed_time(b) for a, b in v) for k, v in evs.items()}
+        # value: the two lanes of every step concurrently, one stream each, as
+        # the server runs them; a step is timed from its first launch to the
+        # end of its slower lane
+        lane_streams = {k: torch.cuda.Stream(device=dev) for k in kinds}
+        for per in passes:
+            for k, (ps, _) in per.items():
+                ps.stream = lane_streams[k]
+        s0 = lane_streams[next(iter(kinds))]
+
+        def concurrent_step(i, evpair=None):
+            per = passes[i % len(passes)]
+            start = torch.cuda.Event(enable_timing=evpair is not None)
+            start.record(s0)
+            for k, (ps, _) in per.items():
+                lane_streams[k].wait_event(start)
+                ps.run()
+            for k in per:
+                if lane_streams[k] is not s0:
+                    done = torch.cuda.Event()
+                    done.record(lane_streams[k])
+                    s0.wait_event(done)
+            if evpair is not None:
+                end = torch.cuda.Event(enable_timing=True)
+                end.record(s0)
+                evpair.append((start, end))
+
+        for i in range(args.warmup):
+            concurrent_step(i)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        steps_ev = []
+        l0 = lds.launch_count()
+        t_c = time.time()
+        for i in range(K):
+            concurrent_step(i, steps_ev)
+        torch.cuda.synchronize()
+        windows.append((t_c, time.time()))
         launches = lds.launch_count() - l0
         for ps, _ in passes[0].values():
             ps.sync_status()
-        ms = {k: sum(a.elapsed_time(b) for a, b in v) for k, v in evs.items()}
         step_atoms = [sum(r.n_atoms for r in st) for st in steps]
         atoms_timed = sum(step_atoms[i % len(steps)] for i in range(K))
-        value, tot_ms, _ = replica_throughput(atoms_timed, sum(ms.values()), dist, dev)
+        value, tot_ms, _ = replica_throughput(atoms_timed, sum(a.elapsed_time(b) for a, b in steps_ev), dist, dev)
         flops_timed = {k: sum(per[k][1] for i in range(K) for per in [passes[i % len(passes)]] if k in per)
                        for k in kinds}
         bs_atoms_timed = sum(sum(r.n_atoms for r in steps[i % len(steps)] if r.lane == "bs") for i in range(K))
@@ -521,13 +562,15 @@ def run_serve(args, torch, lds, dev, world, rank, local, dist):
             "traffic_note": "bytes per step of the bispectrum lane, ncu DRAM bytes per atom of the 8192-atom "
                             "launch (profiles/) times the lane's atoms per step",
             "kernel": BS_KERNELS + " (bispectrum 2J=8 lane of the batched pass)",
-            "flops_per_step": flops_timed["bs"] / K, "share_of_pass_time": ms.get("bs", 0.0) / tot_ms,
+            "flops_per_step": flops_timed["bs"] / K, "share_of_pass_time": ms.get("bs", 0.0) / sum(ms.values()),
+            "timing": "per-lane CUDA events with the lanes in turn on one stream (K steps before the "
+                      "concurrent steps that give value)",
             "flop_count": "libdescriptor_b200/flops.py: U recursion + Z/B/Y + the reverse-mode pair sweep",
             "peak_source": "bench.py FP64 FMA probe (ld_measure_fp64_peak), same run; MEASURED_PEAKS.json has no "
                            "FP64 figure",
             "call_weights_flops": {k: round(v, 1) for k, v in weights.items()},
             "sf_lane": {"achieved": ach_sf, "frac": ach_sf / peak, "kernel": "sfg_kernel<1,1,0>",
-                        "share_of_pass_time": ms.get("sf", 0.0) / tot_ms}}
+                        "share_of_pass_time": ms.get("sf", 0.0) / sum(ms.values())}}
     cpu, parity = None, None
     if not args.no_cpu_baseline and world == 1:
         r, sample, thr, fwd, outs = mix_cpu(specs, reqs[:REQ_PER_STEP], budget_s=12.0)
@@ -564,7 +607,8 @@ def run_serve(args, torch, lds, dev, world, rank, local, dist):
              "density": 0.05, "d_min": 2.0, "cutoff": 5.0, "mix": MIX, "hbm_budget_gb": 40,
              "stream_setup_s": round(gen_s, 1),
              "l2": "inputs of every step (>= 100 MB per lane pass) exceed the 126 MB L2 footprint reuse; no flush",
-             "value": "batched resident pass (one launch per lane per step, inputs in HBM)",
+             "value": "batched resident pass (one launch per lane per step, the two lanes concurrently on "
+                      "their own streams, inputs in HBM)",
              "parallelism": f"replicas x{world}"}
     return {
         "metric": METRIC, "value": value, "unit": "atoms/s", "n_gpus": world, "steps": K, "warmup": args.warmup,
@@ -634,13 +678,44 @@ def run_batch512(args, torch, lds, dev, world, rank, local, dist):
                     e1.record(stream)
                     evs[k].append((e0, e1))
         torch.cuda.synchronize()
+        # value: both descriptors' graphs concurrently, one stream each; a step
+        # is timed from its first replay to the end of the slower one (the
+        # per-descriptor times above, graphs in turn, give the roofline)
+        streams = {k: (stream if i == 0 else torch.cuda.Stream(device=dev)) for i, k in enumerate(passes)}
+        for k, ps in passes.items():
+            ps.stream = streams[k]
+
+        def concurrent_step(evpair=None):
+            start = torch.cuda.Event(enable_timing=evpair is not None)
+            start.record(stream)
+            for k, ps in passes.items():
+                streams[k].wait_event(start)
+                ps.replay()
+            for k in passes:
+                if streams[k] is not stream:
+                    done = torch.cuda.Event()
+                    done.record(streams[k])
+                    stream.wait_event(done)
+            if evpair is not None:
+                end = torch.cuda.Event(enable_timing=True)
+                end.record(stream)
+                evpair.append((start, end))
+
+        for _ in range(args.warmup):
+            concurrent_step()
+        torch.cuda.synchronize()
+        steps_ev = []
+        for _ in range(args.steps):
+            concurrent_step(steps_ev)
+        torch.cuda.synchronize()
         t_b = time.time()
     for ps in passes.values():
         ps.sync_status()
-    # graph replays: count kernels per captured pass
+    # graph replays: count kernels per captured pass (the concurrent steps)
     launches = sum(ps.launches_per_pass for ps in passes.values()) * args.steps
     ms = {k: sum(a.elapsed_time(b_) for a, b_ in v) / args.steps for k, v in evs.items()}
-    value, step_ms, _ = replica_throughput(n_rows, sum(ms.values()), dist, dev)
+    conc_ms = sum(a.elapsed_time(b_) for a, b_ in steps_ev) / args.steps
+    value, step_ms, _ = replica_throughput(n_rows, conc_ms, dist, dev)
     # e2e through the batch API: the host batch (pinned, as a server keeps its
     # buffers) uploaded once for both descriptors, one pass per descriptor,
     # descriptors and forces read back into pinned host buffers, every step;
@@ -730,7 +805,8 @@ def run_batch512(args, torch, lds, dev, world, rank, local, dist):
     ach = flop[dom] / (ms[dom] * 1e-3) / 1e12
     roof = {"bound": "fp64", "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak, "traffic": None,
             "kernel": f"{dom} batched pass", "flops_per_step": flop[dom],
-            "share_of_step_time": ms[dom] / step_ms,
+            "share_of_step_time": ms[dom] / sum(ms.values()),
+            "timing": "per-descriptor graph replays in turn (before the concurrent steps that give value)",
             "peak_source": "bench.py FP64 FMA probe (ld_measure_fp64_peak), same run"}
     cpu, parity = None, None
     if not args.no_cpu_baseline and world == 1:
@@ -759,7 +835,7 @@ def run_batch512(args, torch, lds, dev, world, rank, local, dist):
     cdesc = {"workload": "batched_512_diamond_cells_sf24_and_bs2J6", "cells": 512, "atoms": int(n_rows),
              "n_cells_per_axis": "U{1..6}", "strain": 0.03, "jitter": 0.1, "cutoff": 5.0,
              "tuned_launch_shape": chosen,
-             "per_config_loop_ms": loop_ms, "graph_pass_ms": ms,
+             "per_config_loop_ms": loop_ms, "graph_pass_ms": ms, "concurrent_step_ms": conc_ms,
              "per_config_loop_atoms_per_s": world * n_rows / (sum(loop_ms.values()) * 1e-3),
              "l2": "inputs exceed L2 (549,722 coordinate rows, ~20 MB neighbour lists, 100+ MB dL/d(desc)); no flush",
              "parallelism": f"replicas x{world}"}

@@ -270,6 +270,25 @@ int ld_stage_request(int n_atoms, int n_total, long long nnz, int width,
                      int *d_centre, long long *d_begin, int *d_counts, double *d_dE,
                      ld_stream stream);
 
+/* The two halves of ld_stage_request, for a runtime that packs several
+ * requests on host threads at once and then enqueues their uploads in
+ * admission order (no reference counterpart).  ld_stage_pack writes the
+ * request into `staging` exactly as ld_stage_request does (indices rebased
+ * and checked) on the calling thread only and touches no device: calls for
+ * different requests and staging areas may run concurrently.
+ * ld_stage_upload enqueues the uploads of a packed staging area on
+ * `stream`, with the same slots and sizes as its ld_stage_pack. */
+int ld_stage_pack(int n_atoms, int n_total, long long nnz, int width,
+                  int row0, int atom0, long long entry0,
+                  const double *coords, const int *species, const int *image,
+                  const int *neighbor_list, const int *number_of_neighs,
+                  const double *dE_ddesc, void *staging, size_t staging_bytes);
+int ld_stage_upload(int n_atoms, int n_total, long long nnz, int width,
+                    int row0, int atom0, long long entry0, void *staging, size_t staging_bytes,
+                    double *d_coords, int *d_species, int *d_image, int *d_nbl,
+                    int *d_centre, long long *d_begin, int *d_counts, double *d_dE,
+                    ld_stream stream);
+
 /* Descriptor + VJP pass that allocates no device memory (no counterpart in
  * the reference; it serves callers that cannot call cudaMalloc while they
  * evaluate forces, e.g. engines whose device memory is owned by their own

@@ -423,6 +423,29 @@ PYBIND11_MODULE(_libdescriptor, m) {
         }
         check(rc);
     });
+    m.def("_stage_pack", [](int n, int nt, long long nnz, int width, int row0, int atom0, long long entry0,
+                            DArr coords, IArr species, IArr image, IArr nbl, IArr counts, DArr dE,
+                            std::uintptr_t staging, std::size_t staging_bytes) {
+        if ((long long)coords.size() < 3LL * nt || (long long)species.size() < nt || (long long)image.size() < nt ||
+            (long long)nbl.size() < nnz || (long long)counts.size() < n || (long long)dE.size() < (long long)n * width)
+            throw py::value_error("_stage_pack: arrays shorter than the stated sizes");
+        int rc;
+        {
+            py::gil_scoped_release nogil;
+            rc = ld_stage_pack(n, nt, nnz, width, row0, atom0, entry0, coords.data(), species.data(), image.data(),
+                               nnz ? nbl.data() : nullptr, counts.data(), dE.data(), (void *)staging, staging_bytes);
+        }
+        check(rc);
+    });
+    m.def("_stage_upload", [](int n, int nt, long long nnz, int width, int row0, int atom0, long long entry0,
+                              std::uintptr_t staging, std::size_t staging_bytes, std::uintptr_t d_coords,
+                              std::uintptr_t d_species, std::uintptr_t d_image, std::uintptr_t d_nbl,
+                              std::uintptr_t d_centre, std::uintptr_t d_begin, std::uintptr_t d_counts,
+                              std::uintptr_t d_dE, std::uintptr_t stream) {
+        check(ld_stage_upload(n, nt, nnz, width, row0, atom0, entry0, (void *)staging, staging_bytes,
+                              (double *)d_coords, (int *)d_species, (int *)d_image, (int *)d_nbl, (int *)d_centre,
+                              (long long *)d_begin, (int *)d_counts, (double *)d_dE, (ld_stream)stream));
+    });
     m.def("_create_paddings_dev", [](double cutoff, DArr cell, IArr pbc, std::uintptr_t coords, std::uintptr_t species,
                                      int n_atoms, int max_pad, std::uintptr_t pc, std::uintptr_t ps, std::uintptr_t pi,
                                      std::uintptr_t stream) {

@@ -51,42 +51,58 @@ extern "C" int ld_stage_bytes(int n_atoms, int n_total, long long nnz, int width
     return LD_OK;
 }
 
-extern "C" int ld_stage_request(int n_atoms, int n_total, long long nnz, int width, int row0, int atom0,
-                                long long entry0, const double *coords, const int *species, const int *image,
-                                const int *neighbor_list, const int *number_of_neighs, const double *dE_ddesc,
-                                void *staging, size_t staging_bytes, double *d_coords, int *d_species,
-                                int *d_image, int *d_nbl, int *d_centre, long long *d_begin, int *d_counts,
-                                double *d_dE, ld_stream stream) {
+namespace {
+
+struct Fields {
+    double *coords;
+    int *species, *image, *nbl, *centre;
+    long long *begin;
+    int *counts;
+    double *dE;
+};
+
+Fields fields(void *staging, const StageLayout &L) {
+    char *b = static_cast<char *>(staging);
+    return {reinterpret_cast<double *>(b + L.off[0]), reinterpret_cast<int *>(b + L.off[1]),
+            reinterpret_cast<int *>(b + L.off[2]),    reinterpret_cast<int *>(b + L.off[3]),
+            reinterpret_cast<int *>(b + L.off[4]),    reinterpret_cast<long long *>(b + L.off[5]),
+            reinterpret_cast<int *>(b + L.off[6]),    reinterpret_cast<double *>(b + L.off[7])};
+}
+
+int check_staging(void *staging, size_t staging_bytes, const StageLayout &L, const char *who) {
+    using namespace ldb;
+    if (!staging) return fail(LD_ERR_INVALID_ARG, std::string(who) + ": staging is NULL");
+    if (reinterpret_cast<std::uintptr_t>(staging) % kAlign)
+        return fail(LD_ERR_INVALID_ARG, std::string(who) + ": staging must be 256-byte aligned");
+    if (staging_bytes < L.total)
+        return fail(LD_ERR_INVALID_ARG, std::string(who) + ": staging of " + std::to_string(staging_bytes) +
+                                            " bytes < " + std::to_string(L.total) + " needed");
+    return LD_OK;
+}
+
+// The host half of staging: every field of the request into the staging
+// layout, indices rebased and range-checked.  max_threads 0: one host
+// thread per MiB of copying, up to the cores (at most 16); 1: this thread.
+int stage_pack(int n_atoms, int n_total, long long nnz, int width, int row0, int atom0, long long entry0,
+               const double *coords, const int *species, const int *image, const int *neighbor_list,
+               const int *number_of_neighs, const double *dE_ddesc, void *staging, size_t staging_bytes,
+               int max_threads, const char *who) {
     using namespace ldb;
     if (n_atoms <= 0 || n_total < n_atoms || nnz < 0 || width <= 0 || row0 < 0 || atom0 < 0 || entry0 < 0)
-        return fail(LD_ERR_INVALID_ARG, "ld_stage_request: bad sizes or slots");
-    if (!coords || !species || !image || !number_of_neighs || !dE_ddesc || (nnz > 0 && !neighbor_list) ||
-        !staging || !d_coords || !d_species || !d_image || (nnz > 0 && !d_nbl) || !d_centre || !d_begin ||
-        !d_counts || !d_dE)
-        return fail(LD_ERR_INVALID_ARG, "ld_stage_request: NULL array");
-    if (reinterpret_cast<std::uintptr_t>(staging) % kAlign)
-        return fail(LD_ERR_INVALID_ARG, "ld_stage_request: staging must be 256-byte aligned");
+        return fail(LD_ERR_INVALID_ARG, std::string(who) + ": bad sizes or slots");
+    if (!coords || !species || !image || !number_of_neighs || !dE_ddesc || (nnz > 0 && !neighbor_list))
+        return fail(LD_ERR_INVALID_ARG, std::string(who) + ": NULL array");
     const StageLayout L = layout(n_atoms, n_total, nnz, width);
-    if (staging_bytes < L.total)
-        return fail(LD_ERR_INVALID_ARG, "ld_stage_request: staging of " + std::to_string(staging_bytes) +
-                                            " bytes < " + std::to_string(L.total) + " needed");
-    char *b = static_cast<char *>(staging);
-    double *s_coords = reinterpret_cast<double *>(b + L.off[0]);
-    int *s_species = reinterpret_cast<int *>(b + L.off[1]);
-    int *s_image = reinterpret_cast<int *>(b + L.off[2]);
-    int *s_nbl = reinterpret_cast<int *>(b + L.off[3]);
-    int *s_centre = reinterpret_cast<int *>(b + L.off[4]);
-    long long *s_begin = reinterpret_cast<long long *>(b + L.off[5]);
-    int *s_counts = reinterpret_cast<int *>(b + L.off[6]);
-    double *s_dE = reinterpret_cast<double *>(b + L.off[7]);
+    if (int rc = check_staging(staging, staging_bytes, L, who)) return rc;
+    const Fields F = fields(staging, L);
 
     // row arrays (sequential prefix) + count check
     long long pos = entry0;
     for (int j = 0; j < n_atoms; ++j) {
         const int c = number_of_neighs[j];
         if (c < 0) return fail(LD_ERR_INVALID_ARG, "negative neighbour count");
-        s_centre[j] = atom0 + j;
-        s_begin[j] = pos;
+        F.centre[j] = atom0 + j;
+        F.begin[j] = pos;
         pos += c;
     }
     if (pos - entry0 != nnz) return fail(LD_ERR_INVALID_ARG, "neighbour counts do not add up to nnz");
@@ -101,12 +117,12 @@ extern "C" int ld_stage_request(int n_atoms, int n_total, long long nnz, int wid
         bool rebase;
     };
     Job jobs[6] = {
-        {(char *)s_coords, (const char *)coords, (long long)n_total * 24, 0, 0, false},
-        {(char *)s_species, (const char *)species, (long long)n_total * 4, 0, 0, false},
-        {(char *)s_counts, (const char *)number_of_neighs, (long long)n_atoms * 4, 0, 0, false},
-        {(char *)s_dE, (const char *)dE_ddesc, (long long)n_atoms * width * 8, 0, 0, false},
-        {(char *)s_image, (const char *)image, (long long)n_total, row0, n_atoms, true},
-        {(char *)s_nbl, (const char *)neighbor_list, nnz, atom0, n_total, true},
+        {(char *)F.coords, (const char *)coords, (long long)n_total * 24, 0, 0, false},
+        {(char *)F.species, (const char *)species, (long long)n_total * 4, 0, 0, false},
+        {(char *)F.counts, (const char *)number_of_neighs, (long long)n_atoms * 4, 0, 0, false},
+        {(char *)F.dE, (const char *)dE_ddesc, (long long)n_atoms * width * 8, 0, 0, false},
+        {(char *)F.image, (const char *)image, (long long)n_total, row0, n_atoms, true},
+        {(char *)F.nbl, (const char *)neighbor_list, nnz, atom0, n_total, true},
     };
     constexpr long long kChunkBytes = 1 << 20;
     struct Piece {
@@ -124,9 +140,9 @@ extern "C" int ld_stage_request(int n_atoms, int n_total, long long nnz, int wid
     }
     int bad = 0;
     const int np = (int)pieces.size();
-    // one host thread per MiB of copying, up to the cores (at most 16)
     static const int kCores = std::max(1, std::min(16, (int)std::thread::hardware_concurrency()));
-    const int nthr = (int)std::max(1LL, std::min<long long>(kCores, total / kChunkBytes));
+    const int cap = max_threads > 0 ? std::min(max_threads, kCores) : kCores;
+    const int nthr = (int)std::max(1LL, std::min<long long>(cap, total / kChunkBytes));
 #pragma omp parallel for num_threads(nthr) schedule(dynamic, 1) reduction(| : bad) if (nthr > 1)
     for (int i = 0; i < np; ++i) {
         const Piece &pc = pieces[i];
@@ -146,16 +162,65 @@ extern "C" int ld_stage_request(int n_atoms, int n_total, long long nnz, int wid
         }
     }
     if (bad) return fail(LD_ERR_INVALID_ARG, "an image or neighbour index lies outside the request's atoms");
+    return LD_OK;
+}
 
+// The device half: one upload per field of a packed staging area.
+int stage_upload(int n_atoms, int n_total, long long nnz, int width, int row0, int atom0, long long entry0,
+                 void *staging, size_t staging_bytes, double *d_coords, int *d_species, int *d_image, int *d_nbl,
+                 int *d_centre, long long *d_begin, int *d_counts, double *d_dE, ld_stream stream,
+                 const char *who) {
+    using namespace ldb;
+    if (n_atoms <= 0 || n_total < n_atoms || nnz < 0 || width <= 0 || row0 < 0 || atom0 < 0 || entry0 < 0)
+        return fail(LD_ERR_INVALID_ARG, std::string(who) + ": bad sizes or slots");
+    if (!d_coords || !d_species || !d_image || (nnz > 0 && !d_nbl) || !d_centre || !d_begin || !d_counts || !d_dE)
+        return fail(LD_ERR_INVALID_ARG, std::string(who) + ": NULL device array");
+    const StageLayout L = layout(n_atoms, n_total, nnz, width);
+    if (int rc = check_staging(staging, staging_bytes, L, who)) return rc;
+    const Fields F = fields(staging, L);
     cudaStream_t s = (cudaStream_t)stream;
     const auto h2d = cudaMemcpyHostToDevice;
-    LDB_CUDA(cudaMemcpyAsync(d_coords + 3 * (size_t)atom0, s_coords, (size_t)n_total * 24, h2d, s));
-    LDB_CUDA(cudaMemcpyAsync(d_species + atom0, s_species, (size_t)n_total * 4, h2d, s));
-    LDB_CUDA(cudaMemcpyAsync(d_image + atom0, s_image, (size_t)n_total * 4, h2d, s));
-    if (nnz > 0) LDB_CUDA(cudaMemcpyAsync(d_nbl + entry0, s_nbl, (size_t)nnz * 4, h2d, s));
-    LDB_CUDA(cudaMemcpyAsync(d_centre + row0, s_centre, (size_t)n_atoms * 4, h2d, s));
-    LDB_CUDA(cudaMemcpyAsync(d_begin + row0, s_begin, (size_t)n_atoms * 8, h2d, s));
-    LDB_CUDA(cudaMemcpyAsync(d_counts + row0, s_counts, (size_t)n_atoms * 4, h2d, s));
-    LDB_CUDA(cudaMemcpyAsync(d_dE + (size_t)row0 * width, s_dE, (size_t)n_atoms * width * 8, h2d, s));
+    LDB_CUDA(cudaMemcpyAsync(d_coords + 3 * (size_t)atom0, F.coords, (size_t)n_total * 24, h2d, s));
+    LDB_CUDA(cudaMemcpyAsync(d_species + atom0, F.species, (size_t)n_total * 4, h2d, s));
+    LDB_CUDA(cudaMemcpyAsync(d_image + atom0, F.image, (size_t)n_total * 4, h2d, s));
+    if (nnz > 0) LDB_CUDA(cudaMemcpyAsync(d_nbl + entry0, F.nbl, (size_t)nnz * 4, h2d, s));
+    LDB_CUDA(cudaMemcpyAsync(d_centre + row0, F.centre, (size_t)n_atoms * 4, h2d, s));
+    LDB_CUDA(cudaMemcpyAsync(d_begin + row0, F.begin, (size_t)n_atoms * 8, h2d, s));
+    LDB_CUDA(cudaMemcpyAsync(d_counts + row0, F.counts, (size_t)n_atoms * 4, h2d, s));
+    LDB_CUDA(cudaMemcpyAsync(d_dE + (size_t)row0 * width, F.dE, (size_t)n_atoms * width * 8, h2d, s));
     return LD_OK;
+}
+
+}  // namespace
+
+extern "C" int ld_stage_request(int n_atoms, int n_total, long long nnz, int width, int row0, int atom0,
+                                long long entry0, const double *coords, const int *species, const int *image,
+                                const int *neighbor_list, const int *number_of_neighs, const double *dE_ddesc,
+                                void *staging, size_t staging_bytes, double *d_coords, int *d_species,
+                                int *d_image, int *d_nbl, int *d_centre, long long *d_begin, int *d_counts,
+                                double *d_dE, ld_stream stream) {
+    using namespace ldb;
+    if (!d_coords || !d_species || !d_image || (nnz > 0 && !d_nbl) || !d_centre || !d_begin || !d_counts || !d_dE)
+        return fail(LD_ERR_INVALID_ARG, "ld_stage_request: NULL array");
+    int rc = stage_pack(n_atoms, n_total, nnz, width, row0, atom0, entry0, coords, species, image, neighbor_list,
+                        number_of_neighs, dE_ddesc, staging, staging_bytes, 0, "ld_stage_request");
+    if (rc) return rc;
+    return stage_upload(n_atoms, n_total, nnz, width, row0, atom0, entry0, staging, staging_bytes, d_coords,
+                        d_species, d_image, d_nbl, d_centre, d_begin, d_counts, d_dE, stream, "ld_stage_request");
+}
+
+extern "C" int ld_stage_pack(int n_atoms, int n_total, long long nnz, int width, int row0, int atom0,
+                             long long entry0, const double *coords, const int *species, const int *image,
+                             const int *neighbor_list, const int *number_of_neighs, const double *dE_ddesc,
+                             void *staging, size_t staging_bytes) {
+    return stage_pack(n_atoms, n_total, nnz, width, row0, atom0, entry0, coords, species, image, neighbor_list,
+                      number_of_neighs, dE_ddesc, staging, staging_bytes, 1, "ld_stage_pack");
+}
+
+extern "C" int ld_stage_upload(int n_atoms, int n_total, long long nnz, int width, int row0, int atom0,
+                               long long entry0, void *staging, size_t staging_bytes, double *d_coords,
+                               int *d_species, int *d_image, int *d_nbl, int *d_centre, long long *d_begin,
+                               int *d_counts, double *d_dE, ld_stream stream) {
+    return stage_upload(n_atoms, n_total, nnz, width, row0, atom0, entry0, staging, staging_bytes, d_coords,
+                        d_species, d_image, d_nbl, d_centre, d_begin, d_counts, d_dE, stream, "ld_stage_upload");
 }

@@ -13,8 +13,9 @@ and rows (centre, neighbour-list start, count, dL/d(desc), descriptors,
 forces).  A request is *admitted* when contiguous space for its atoms,
 neighbours and rows is free in every ring of its lane (admission by HBM
 footprint, first come first served per lane); its inputs are then written,
-with indices rebased to the ring slots, into a pinned host staging ring and
-copied to the device on the lane's copy stream.
+with indices rebased to the ring slots, into a pinned host staging ring (the
+requests admitted together are packed on a pool of host threads) and copied
+to the device on the lane's copy stream in admission order.
 
 Continuous batching.  While fewer than ``depth`` batches of a lane are on the
 GPU, every admitted request that is not yet launched joins the next batch
@@ -294,6 +295,9 @@ class Scheduler:
                 self.admitted[k].append(req)
                 rows += req.n_atoms
                 n += 1
+        flush = getattr(self.backend, "flush", None)
+        if flush is not None:
+            flush()
         return n
 
     # -- batching -------------------------------------------------------
@@ -421,7 +425,11 @@ class ServingEngine:
 
     def __init__(self, lanes: dict, budget_bytes: int = 40 << 30, shares: dict | None = None,
                  max_batch_rows: int = 1 << 19, depth: int = 2, stage_bytes: int = 512 << 20,
-                 out_rows: int | None = None, device=None, tuning: dict | None = None):
+                 out_rows: int | None = None, device=None, tuning: dict | None = None,
+                 pack_threads: int | None = None):
+        import concurrent.futures
+        import os
+
         import torch
 
         from . import _ext
@@ -448,6 +456,12 @@ class ServingEngine:
         self.caps = caps
         self.launches = 0
         self.host_stage_s = 0.0
+        # host threads that pack admitted requests into pinned staging (the
+        # packing releases the interpreter lock)
+        self._pack_threads = max(1, pack_threads if pack_threads is not None else min(16, os.cpu_count() or 1))
+        self._pool = (concurrent.futures.ThreadPoolExecutor(self._pack_threads, thread_name_prefix="ld-pack")
+                      if self._pack_threads > 1 else None)
+        self._jobs: list = []
         self.t0 = time.perf_counter()
 
     def clock(self) -> float:
@@ -460,8 +474,9 @@ class ServingEngine:
             ln.stage_ring.free(u0)
 
     def stage(self, req: Request) -> None:
-        """Pinned staging + rebased uploads of one admitted request
-        (``ld_stage_request``, native)."""
+        """Reserve pinned staging for one admitted request; ``flush`` packs it
+        (``ld_stage_pack``, native, indices rebased) and uploads it
+        (``ld_stage_upload``)."""
         torch = self.torch
         torch.cuda.nvtx.range_push(f"serve: stage request {req.rid}")
         try:
@@ -470,9 +485,10 @@ class ServingEngine:
             torch.cuda.nvtx.range_pop()
 
     def _stage(self, req: Request) -> None:
-        torch = self.torch
+        """Reserve the request's pinned staging space; the packing and the
+        uploads follow in ``flush`` (packing on host threads, uploads in
+        admission order)."""
         ln = self.lanes[req.lane]
-        r0, a0, e0 = req.slots
         n, nt, nnz, W = req.n_atoms, req.n_total, req.nnz, ln.W
         t_in = time.perf_counter()
         nbytes = int(self._ext._stage_bytes(n, nt, nnz, W))
@@ -480,21 +496,60 @@ class ServingEngine:
         self._reclaim_staging(ln)
         u0 = ln.stage_ring.alloc(units)
         while u0 is None:
-            # staging full: wait for the oldest upload
+            # staging full: upload what is packed, then wait for the oldest upload
+            if any(job[1] is ln for job in self._jobs):
+                self.flush()
             if not ln.staged:
                 raise RuntimeError("request larger than the pinned staging ring")
             ln.staged[0][1].synchronize()
             self._reclaim_staging(ln)
             u0 = ln.stage_ring.alloc(units)
-        self._ext._stage_request(n, nt, nnz, W, r0, a0, e0, req.coords, req.species, req.image, req.nbl,
-                                 req.counts, req.dE, ln.stage.data_ptr() + 256 * u0, units * 256,
-                                 ln.coords.data_ptr(), ln.species.data_ptr(), ln.image.data_ptr(),
-                                 ln.nbl.data_ptr(), ln.centre.data_ptr(), ln.begin.data_ptr(),
-                                 ln.counts.data_ptr(), ln.dE.data_ptr(), ln.s_h2d.cuda_stream)
-        ev = torch.cuda.Event()
-        ev.record(ln.s_h2d)
-        ln.staged.append((u0, ev))
-        req.staged = ev
+        self._jobs.append((req, ln, u0, units, nbytes))
+        self.host_stage_s += time.perf_counter() - t_in
+
+    def _pack(self, job) -> None:
+        req, ln, u0, units, _ = job
+        r0, a0, e0 = req.slots
+        self._ext._stage_pack(req.n_atoms, req.n_total, req.nnz, ln.W, r0, a0, e0, req.coords, req.species,
+                              req.image, req.nbl, req.counts, req.dE, ln.stage.data_ptr() + 256 * u0, units * 256)
+
+    def _pack_group(self, jobs) -> None:
+        for job in jobs:
+            self._pack(job)
+
+    def flush(self) -> None:
+        """Pack the reserved requests into pinned staging, spread over host
+        threads when there is enough to copy, then enqueue their uploads and
+        mark each with an event, in admission order."""
+        if not self._jobs:
+            return
+        torch = self.torch
+        t_in = time.perf_counter()
+        jobs, self._jobs = self._jobs, []
+        total = sum(j[4] for j in jobs)
+        if self._pool is None or len(jobs) == 1 or total < (4 << 20):
+            self._pack_group(jobs)
+        else:
+            # longest first onto the least loaded of the workers
+            groups = [[] for _ in range(min(self._pack_threads, len(jobs)))]
+            load = [0] * len(groups)
+            for job in sorted(jobs, key=lambda j: -j[4]):
+                g = load.index(min(load))
+                groups[g].append(job)
+                load[g] += job[4]
+            for f in [self._pool.submit(self._pack_group, g) for g in groups]:
+                f.result()
+        for req, ln, u0, units, _ in jobs:
+            r0, a0, e0 = req.slots
+            self._ext._stage_upload(req.n_atoms, req.n_total, req.nnz, ln.W, r0, a0, e0,
+                                    ln.stage.data_ptr() + 256 * u0, units * 256, ln.coords.data_ptr(),
+                                    ln.species.data_ptr(), ln.image.data_ptr(), ln.nbl.data_ptr(),
+                                    ln.centre.data_ptr(), ln.begin.data_ptr(), ln.counts.data_ptr(),
+                                    ln.dE.data_ptr(), ln.s_h2d.cuda_stream)
+            ev = torch.cuda.Event()
+            ev.record(ln.s_h2d)
+            ln.staged.append((u0, ev))
+            req.staged = ev
         self.host_stage_s += time.perf_counter() - t_in
 
     def launch(self, plan: BatchPlan) -> None:

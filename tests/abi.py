@@ -97,6 +97,8 @@ class Abi:
             L.ld_stage_request.argtypes = [C.c_int, C.c_int, C.c_longlong, C.c_int, C.c_int, C.c_int,
                                            C.c_longlong, _dp, _ip, _ip, _ip, _ip, _dp, C.c_void_p, C.c_size_t]
             L.ld_stage_request.argtypes += [C.c_void_p] * 9
+            L.ld_stage_pack.argtypes = [C.c_int, C.c_int, C.c_longlong, C.c_int, C.c_int, C.c_int,
+                                        C.c_longlong, _dp, _ip, _ip, _ip, _ip, _dp, C.c_void_p, C.c_size_t]
             L.ld_set_tuning.argtypes = [C.c_void_p, C.c_int, C.c_int]
             L.ld_get_tuning.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
             cls._lib = L

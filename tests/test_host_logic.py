@@ -338,6 +338,32 @@ def test_stage_request_rebases_indices_into_staging():
     np.testing.assert_array_equal(v(7, np.float64, 2 * n), dE.ravel())
 
 
+def test_stage_pack_writes_what_stage_request_writes():
+    """ld_stage_pack, the host half the serving engine runs on its packing
+    threads, fills the staging area byte for byte as ld_stage_request does
+    (and touches no device: it succeeds without one)."""
+    import ctypes as C
+
+    from abi import Abi
+
+    n, nt = 3, 5
+    counts, nbl, image = [2, 0, 3], [1, 4, 0, 2, 3], [0, 1, 2, 0, 2]
+    _, want, coords, species, dE = _stage(n, nt, nbl, counts, image)
+    L = Abi.lib()
+    nb = C.c_size_t()
+    Abi.check(L.ld_stage_bytes(n, nt, len(nbl), 2, C.byref(nb)))
+    raw = np.zeros(nb.value + 512, np.uint8)
+    base = (raw.ctypes.data + 255) & ~255
+    Abi.check(L.ld_stage_pack(n, nt, len(nbl), 2, 5, 100, 1000, np.ascontiguousarray(coords).ravel(), species,
+                              np.asarray(image, np.int32), np.asarray(nbl, np.int32), np.asarray(counts, np.int32),
+                              dE.ravel(), C.c_void_p(base), nb.value))
+    got = raw[base - raw.ctypes.data:][:nb.value]
+    np.testing.assert_array_equal(got, want[:nb.value])
+    assert L.ld_stage_pack(n, nt, len(nbl), 2, 5, 100, 1000, np.ascontiguousarray(coords).ravel(), species,
+                           np.asarray([0, 1, 2, 3, 2], np.int32), np.asarray(nbl, np.int32),
+                           np.asarray(counts, np.int32), dE.ravel(), C.c_void_p(base), nb.value) == 2
+
+
 @pytest.mark.parametrize("bad", ["nbl", "image", "counts"])
 def test_stage_request_rejects_bad_indices(bad):
     from abi import Abi
