@@ -542,6 +542,7 @@ def run_serve(args, torch, lds, dev, world, rank, local, dist):
                             on_done=keep_first_step if rate == max(RATES) else None)
             windows.append((t_b, time.time()))
             served[rate] = res
+        eng.close()
         del eng
         torch.cuda.empty_cache()
         for rate in sorted(RATES):
@@ -802,6 +803,7 @@ def run_batch512(args, torch, lds, dev, world, rank, local, dist):
     t0 = time.perf_counter()
     st = eng.serve(reqs, None)
     serve_s = time.perf_counter() - t0
+    eng.close()
     if rank != 0:
         return None
     flop = {k: sum(algorithmic_flops(specs[k], c, weights) for c in cfgs) for k in specs}

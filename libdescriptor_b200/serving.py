@@ -467,6 +467,18 @@ class ServingEngine:
     def clock(self) -> float:
         return time.perf_counter() - self.t0
 
+    def close(self) -> None:
+        """Stop the packing threads (the device rings go with the engine)."""
+        if self._pool is not None:
+            self._pool.shutdown(wait=True)
+            self._pool = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
     # -- backend interface --------------------------------------------------
     def _reclaim_staging(self, ln: _Lane) -> None:
         while ln.staged and ln.staged[0][1].query():
