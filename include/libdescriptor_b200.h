@@ -388,6 +388,14 @@ long long ld_alloc_count(void);
  * nothing is asked of the device, and the handle stays usable afterwards. */
 int ld_fail_next_allocation(int k);
 
+/* Test hook (no reference counterpart): from now on every new device
+ * allocation of the library -- grow-only buffers and scratch-pool blocks -- is
+ * filled with `byte` (0..255; 0xff makes every double a NaN) before use, so
+ * that a read of memory no kernel wrote shows on every run instead of
+ * depending on what the memory held before; -1 (the default) switches it
+ * off.  Costs one memset per allocation while on. */
+int ld_debug_fill_scratch(int byte);
+
 /* Pinned (page-locked) host memory for results: the device writes into it at
  * the link's rate, where a copy into fresh pageable memory runs several
  * times slower.  Blocks are rounded up to 64 KiB; a released block is kept

@@ -55,6 +55,12 @@ int count_alloc() {
     return LD_OK;
 }
 
+// Test hook: a byte (0..255) that every new device allocation of the library
+// is filled with, so that a kernel reading memory nobody wrote sees garbage
+// (0xff: NaN doubles) on every run; -1 leaves allocations as they come.
+static std::atomic<int> g_fill{-1};
+int scratch_fill() { return g_fill.load(); }
+
 int DevBuf::ensure(size_t n) {
     if (n <= bytes && p) return LD_OK;
     release();
@@ -67,6 +73,8 @@ int DevBuf::ensure(size_t n) {
         return cuda_fail(e, "cudaMalloc");
     }
     bytes = want;
+    const int f = scratch_fill();
+    if (f >= 0) LDB_CUDA(cudaMemset(p, f, want));
     return LD_OK;
 }
 void DevBuf::release() {
@@ -694,7 +702,9 @@ static int build_bs_impl(ld_descriptor *d, double rfac0, int J, int style, doubl
                 zg.push_back(q < nc && mb1 >= 0 && mb1 <= j1 ? cg[cgoff[t] + mb1 * (j2 + 1) + mb] : 0.0);
             }
     }
-    auto zsched = [&](const std::set<int> &need, std::vector<int> &zoff, std::vector<int> &zitem,
+    // with_y: every layer gets items, also layers without needed triples,
+    // whose items write zero Y rows (the pair kernel reads Y of all layers)
+    auto zsched = [&](const std::set<int> &need, bool with_y, std::vector<int> &zoff, std::vector<int> &zitem,
                       std::vector<int> &ztoff, std::vector<int4> &ztl) {
         ztoff.assign(J + 2, 0);
         ztl.clear();
@@ -708,7 +718,7 @@ static int build_bs_impl(ld_descriptor *d, double rfac0, int J, int style, doubl
                 ztl.push_back(make_int4(j1 | (j2 << 8) | (c << 16), gofs[t], cgoff[t], t | ((tslot[t] + 1) << 16)));
             }
             const int t0 = ztoff[j], t1 = (int)ztl.size();
-            if (t1 == t0) continue;
+            if (t1 == t0 && !with_y) continue;
             for (int ma = 0; ma <= j; ++ma) {
                 long long cost = 16;
                 for (int k = t0; k < t1; ++k) {
@@ -742,8 +752,8 @@ static int build_bs_impl(ld_descriptor *d, double rfac0, int J, int style, doubl
     };
     std::vector<int> zoff_f, zitem_f, ztoff_f, zoff_v, zitem_v, ztoff_v;
     std::vector<int4> ztl_f, ztl_v;
-    zsched(need_f, zoff_f, zitem_f, ztoff_f, ztl_f);
-    zsched(need_v, zoff_v, zitem_v, ztoff_v, ztl_v);
+    zsched(need_f, false, zoff_f, zitem_f, ztoff_f, ztl_f);
+    zsched(need_v, true, zoff_v, zitem_v, ztoff_v, ztl_v);
     std::vector<int4> trip4;
     for (auto &t : trip) trip4.push_back(make_int4(t[0], t[1], t[2], t[3]));
     Arena ar;
@@ -1299,6 +1309,12 @@ const char *ld_error_message(void) { return g_err.c_str(); }
 int ld_version(void) { return 10000 * 0 + 100 * 1 + 0; }
 long long ld_launch_count(void) { return g_launches.load(); }
 long long ld_alloc_count(void) { return g_allocs.load(); }
+int ld_debug_fill_scratch(int byte) {
+    if (byte < -1 || byte > 255) return fail(LD_ERR_INVALID_ARG, "ld_debug_fill_scratch: byte outside -1..255");
+    g_fill.store(byte);
+    return LD_OK;
+}
+
 int ld_fail_next_allocation(int k) {
     if (k < 0) return fail(LD_ERR_INVALID_ARG, "ld_fail_next_allocation: k < 0");
     g_fail_in.store(k);

@@ -47,6 +47,8 @@ void count_launch(int n = 1);
 // buffers, the stream-ordered scratch pool) calls this first; it returns
 // LD_ERR_OOM when ld_fail_next_allocation armed a failure for this one.
 int count_alloc();
+// The byte new allocations are filled with (ld_debug_fill_scratch), or -1.
+int scratch_fill();
 // The device a descriptor handle was created on.
 int handle_device(const ld_descriptor *d);
 

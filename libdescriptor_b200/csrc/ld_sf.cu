@@ -42,11 +42,16 @@ sf_kernel(SFDev p, RowArgs a, int per_warp_doubles, int *queue) {
         if (lane == 0) r0 = atomicAdd(queue, 1);
         row = __shfl_sync(0xffffffffu, r0, 0);
     }
+    // the next row's list is copied into the slice (cp.async) while the
+    // current row computes
+    RowMeta nxt{};
+    if (row < a.n_rows) {
+        nxt = row_meta(a, row);
+        csr_prefetch(a, nxt, cap, S.nbl);
+    }
     for (; row < a.n_rows;) {
-        const int i = a.row_centre ? a.row_centre[row] : row;
-        const int lrow = a.row_list ? a.row_list[row] : row;
-        const long long off = a.nbl_begin ? a.nbl_begin[lrow] : a.off[lrow];
-        const int n = (int)(a.off[lrow + 1] - a.off[lrow]);
+        const RowMeta m = nxt;
+        const int i = m.i, n = m.n;
         const int cur_row = row;  // row being processed; `row` is the next one
         // next row: from the shared counter (dynamic) or by grid stride
         if (queue) {
@@ -56,18 +61,21 @@ sf_kernel(SFDev p, RowArgs a, int per_warp_doubles, int *queue) {
         } else {
             row += gridDim.x * nw;
         }
+        if (row < a.n_rows) nxt = row_meta(a, row);
         double *const dco = VJP ? a.dcoords + (size_t)cur_row * a.dc_stride : nullptr;
+        csr_wait();
         if (n > cap || n < 0 || (a.n_total > 0 && (i < 0 || i >= a.n_total))) {
             raise_status(a.status, n > cap ? kDevCapacity : kDevBadIndex);
             if (a.desc)
                 for (int q = lane; q < width; q += 32) a.desc[(size_t)cur_row * width + q] = __longlong_as_double(0x7ff8000000000000LL);
+            if (row < a.n_rows) csr_prefetch(a, nxt, cap, S.nbl);
             continue;
         }
         const double cix = a.coords[3 * i], ciy = a.coords[3 * i + 1], ciz = a.coords[3 * i + 2];
         const int is = a.species[i];
-        // ---- stage the neighbours of this row
+        // ---- stage the neighbours of this row (list from the slice)
         for (int jj = lane; jj < n; jj += 32) {
-            int j = a.nbl[off + jj];
+            int j = S.nbl[jj];
             int ok = 1;
             if (a.n_total > 0 && (j < 0 || j >= a.n_total)) {
                 raise_status(a.status, kDevBadIndex);
@@ -98,6 +106,7 @@ sf_kernel(SFDev p, RowArgs a, int per_warp_doubles, int *queue) {
             }
         }
         __syncwarp();
+        if (row < a.n_rows) csr_prefetch(a, nxt, cap, S.nbl);
         const double *dE = VJP ? a.dE + (size_t)cur_row * width : nullptr;
         double gix = 0.0, giy = 0.0, giz = 0.0;
         // ---- two-body terms (g1, g2, g3)

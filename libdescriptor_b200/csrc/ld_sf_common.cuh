@@ -5,6 +5,7 @@
 
 #include <string>
 
+#include "ld_csr.cuh"
 #include "ld_internal.h"
 
 namespace ldb {
@@ -35,7 +36,7 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 struct WarpSlice {
     double *cx, *cy, *cz, *r, *ir, *rc, *fc, *dfc, *gx, *gy, *gz;
-    int *spec, *idx, *inc;
+    int *spec, *idx, *inc, *nbl;
 };
 
 __device__ __forceinline__ WarpSlice slice(double *base, int cap, bool vjp) {
@@ -59,13 +60,13 @@ __device__ __forceinline__ WarpSlice slice(double *base, int cap, bool vjp) {
     int *q = reinterpret_cast<int *>(p);
     s.spec = q; q += cap;
     s.idx = q; q += cap;
-    s.inc = q;
+    s.inc = q; q += cap;
+    s.nbl = q;
     return s;
 }
 
-
 // Per-warp staging size (doubles; the int arrays are packed after them).
-inline int per_warp_doubles(int cap, bool vjp) { return cap * (vjp ? 11 : 7) + (3 * cap + 1) / 2 + 2; }
+inline int per_warp_doubles(int cap, bool vjp) { return cap * (vjp ? 11 : 7) + (4 * cap + 1) / 2 + 2; }
 
 // Launch a warp-per-centre kernel kern(p, a, per_warp, queue) with the
 // tuned shape: warps per CTA (a.sf_warps), CTA cap per SM, optional dynamic

@@ -66,11 +66,14 @@ sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue)
         if (lane == 0) r0 = atomicAdd(queue, 1);
         row = __shfl_sync(0xffffffffu, r0, 0);
     }
+    RowMeta nxt{};
+    if (row < a.n_rows) {
+        nxt = row_meta(a, row);
+        csr_prefetch(a, nxt, cap, S.nbl);
+    }
     for (; row < a.n_rows;) {
-        const int i = a.row_centre ? a.row_centre[row] : row;
-        const int lrow = a.row_list ? a.row_list[row] : row;
-        const long long off = a.nbl_begin ? a.nbl_begin[lrow] : a.off[lrow];
-        const int n = (int)(a.off[lrow + 1] - a.off[lrow]);
+        const RowMeta m = nxt;
+        const int i = m.i, n = m.n;
         const int cur_row = row;
         if (queue) {
             int r1 = 0;
@@ -79,19 +82,24 @@ sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue)
         } else {
             row += gridDim.x * nw;
         }
+        // the next row's list metadata, loaded now and used once this row's
+        // segment has left the slice
+        if (row < a.n_rows) nxt = row_meta(a, row);
         double *const dco = VJP ? a.dcoords + (size_t)cur_row * a.dc_stride : nullptr;
+        csr_wait();
         if (n > cap || n < 0 || (a.n_total > 0 && (i < 0 || i >= a.n_total))) {
             raise_status(a.status, n > cap ? kDevCapacity : kDevBadIndex);
             if (a.desc)
                 for (int q = lane; q < width; q += 32)
                     a.desc[(size_t)cur_row * width + q] = __longlong_as_double(0x7ff8000000000000LL);
+            if (row < a.n_rows) csr_prefetch(a, nxt, cap, S.nbl);
             continue;
         }
         const double cix = a.coords[3 * i], ciy = a.coords[3 * i + 1], ciz = a.coords[3 * i + 2];
         const int is = a.species[i];
-        // ---- stage the neighbours of this row
+        // ---- stage the neighbours of this row (list from the slice)
         for (int jj = lane; jj < n; jj += 32) {
-            int j = a.nbl[off + jj];
+            int j = S.nbl[jj];
             int ok = 1;
             if (a.n_total > 0 && (j < 0 || j >= a.n_total)) {
                 raise_status(a.status, kDevBadIndex);
@@ -121,6 +129,7 @@ sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue)
             }
         }
         __syncwarp();
+        if (row < a.n_rows) csr_prefetch(a, nxt, cap, S.nbl);
         const double *dE = VJP ? a.dE + (size_t)cur_row * width : nullptr;
         double gix = 0.0, giy = 0.0, giz = 0.0;
         // ---- two-body terms

@@ -92,6 +92,8 @@ int pool_alloc(void **p, size_t bytes, cudaStream_t s) {
     }
     if (int rc = count_alloc()) return rc;
     LDB_CUDA(cudaMallocFromPoolAsync(p, bytes ? bytes : 1, pool, s));
+    const int f = scratch_fill();
+    if (f >= 0) LDB_CUDA(cudaMemsetAsync(*p, f, bytes ? bytes : 1, s));
     return LD_OK;
 }
 

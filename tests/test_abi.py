@@ -132,3 +132,13 @@ def test_allocation_fault_injection_is_host_side():
     assert L.ld_fail_next_allocation(3) == 0
     assert L.ld_fail_next_allocation(0) == 0           # disarmed
     assert L.ld_alloc_count() == n0
+
+
+def test_scratch_fill_hook_checks_its_byte():
+    """ld_debug_fill_scratch takes a byte or -1 (off); arming it touches no
+    device (the GPU test runs the kernels with every allocation filled)."""
+    L = Abi.lib()
+    assert L.ld_debug_fill_scratch(-2) == 2           # LD_ERR_INVALID_ARG
+    assert L.ld_debug_fill_scratch(256) == 2
+    assert L.ld_debug_fill_scratch(0xFF) == 0
+    assert L.ld_debug_fill_scratch(-1) == 0
