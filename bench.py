@@ -453,6 +453,7 @@ def run_serve(args, torch, lds, dev, world, rank, local, dist):
     if dist:
         dist.barrier()
     evs = {k: [] for k in kinds}
+    seq_ev = []
     l0 = lds.launch_count()
     windows = []
     with ClockSampler(local) as clk:
@@ -460,21 +461,28 @@ def run_serve(args, torch, lds, dev, world, rank, local, dist):
         t_a = time.time()
         with torch.cuda.stream(stream):
             for i in range(K):
+                s0_ev = torch.cuda.Event(enable_timing=True)
+                s0_ev.record(stream)
                 for k, (ps, _) in passes[i % len(passes)].items():
                     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                     e0.record(stream)
                     ps.run()
                     e1.record(stream)
                     evs[k].append((e0, e1))
+                s1_ev = torch.cuda.Event(enable_timing=True)
+                s1_ev.record(stream)
+                seq_ev.append((s0_ev, s1_ev))
         torch.cuda.synchronize()
         windows.append((t_a, time.time()))
+        seq_launches = lds.launch_count() - l0
         for ps, _ in passes[0].values():
             ps.sync_status()
         # per-lane kernel times (the roofline's denominators): lanes in turn
         ms = {k: sum(a.elapsed_time(b) for a, b in v) for k, v in evs.items()}
-        # value: the two lanes of every step concurrently, one stream each, as
-        # the server runs them; a step is timed from its first launch to the
-        # end of its slower lane
+        seq_ms = sum(a.elapsed_time(b) for a, b in seq_ev)
+        # the same steps with the two lanes concurrently, one stream each (the
+        # server with overlap_lanes); a step is timed from its first launch to
+        # the end of its slower lane
         lane_streams = {k: torch.cuda.Stream(device=dev) for k in kinds}
         for per in passes:
             for k, (ps, _) in per.items():
@@ -510,12 +518,16 @@ def run_serve(args, torch, lds, dev, world, rank, local, dist):
             concurrent_step(i, steps_ev)
         torch.cuda.synchronize()
         windows.append((t_c, time.time()))
-        launches = lds.launch_count() - l0
+        conc_launches = lds.launch_count() - l0
         for ps, _ in passes[0].values():
             ps.sync_status()
+        conc_ms = sum(a.elapsed_time(b) for a, b in steps_ev)
         step_atoms = [sum(r.n_atoms for r in st) for st in steps]
         atoms_timed = sum(step_atoms[i % len(steps)] for i in range(K))
-        value, tot_ms, _ = replica_throughput(atoms_timed, sum(a.elapsed_time(b) for a, b in steps_ev), dist, dev)
+        # value: the steps as the server issues them (lanes in turn on one
+        # compute stream, or overlapped with --overlap-lanes)
+        launches = conc_launches if args.overlap_lanes else seq_launches
+        value, tot_ms, _ = replica_throughput(atoms_timed, conc_ms if args.overlap_lanes else seq_ms, dist, dev)
         flops_timed = {k: sum(per[k][1] for i in range(K) for per in [passes[i % len(passes)]] if k in per)
                        for k in kinds}
         bs_atoms_timed = sum(sum(r.n_atoms for r in steps[i % len(steps)] if r.lane == "bs") for i in range(K))
@@ -524,7 +536,8 @@ def run_serve(args, torch, lds, dev, world, rank, local, dist):
 
         # ---- e2e: the server over the whole stream at every rate, then the
         # plain per-call path on the same stream at every rate
-        eng = S.ServingEngine(kinds, budget_bytes=40 << 30, shares={"sf": 0.45, "bs": 0.55}, device=dev)
+        eng = S.ServingEngine(kinds, budget_bytes=40 << 30, shares={"sf": 0.45, "bs": 0.55}, device=dev,
+                              overlap_lanes=args.overlap_lanes)
         eng.serve(reqs[:64], None)
         kept = {}                       # results of the first step's requests, top rate
 
@@ -564,8 +577,7 @@ def run_serve(args, torch, lds, dev, world, rank, local, dist):
                             "launch (profiles/) times the lane's atoms per step",
             "kernel": BS_KERNELS + " (bispectrum 2J=8 lane of the batched pass)",
             "flops_per_step": flops_timed["bs"] / K, "share_of_pass_time": ms.get("bs", 0.0) / sum(ms.values()),
-            "timing": "per-lane CUDA events with the lanes in turn on one stream (K steps before the "
-                      "concurrent steps that give value)",
+            "timing": "per-lane CUDA events with the lanes in turn on one stream",
             "flop_count": "libdescriptor_b200/flops.py: U recursion + Z/B/Y + the reverse-mode pair sweep",
             "peak_source": "bench.py FP64 FMA probe (ld_measure_fp64_peak), same run; MEASURED_PEAKS.json has no "
                            "FP64 figure",
@@ -608,8 +620,11 @@ def run_serve(args, torch, lds, dev, world, rank, local, dist):
              "density": 0.05, "d_min": 2.0, "cutoff": 5.0, "mix": MIX, "hbm_budget_gb": 40,
              "stream_setup_s": round(gen_s, 1),
              "l2": "inputs of every step (>= 100 MB per lane pass) exceed the 126 MB L2 footprint reuse; no flush",
-             "value": "batched resident pass (one launch per lane per step, the two lanes concurrently on "
-                      "their own streams, inputs in HBM)",
+             "value": "batched resident pass (one launch per lane per step, inputs in HBM), "
+                      + ("the two lanes concurrently on their own streams" if args.overlap_lanes
+                         else "the lanes in turn on one compute stream") + ", as the server issues them",
+             "step_ms": {"lanes_in_turn": seq_ms / K, "lanes_overlapped": conc_ms / K},
+             "server_overlap_lanes": bool(args.overlap_lanes),
              "parallelism": f"replicas x{world}"}
     return {
         "metric": METRIC, "value": value, "unit": "atoms/s", "n_gpus": world, "steps": K, "warmup": args.warmup,
@@ -1062,6 +1077,9 @@ def main():
     ap.add_argument("--workload", default="serve", choices=["serve", "batch512", "bs8", "sf24"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--overlap-lanes", action="store_true",
+                    help="serve: each lane's kernels on its own stream (value and server), instead of the lanes "
+                         "in turn on one compute stream")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.steps is None:

@@ -23,8 +23,9 @@ GPU, every admitted request that is not yet launched joins the next batch
 ``ld_gradient_rows_dev`` launch over rows that are contiguous in the row ring;
 the neighbour-list starts are per row, so nothing is gathered.  Requests
 arriving while batches run are admitted as memory frees and join the next
-batch; the two lanes run on their own streams, so symmetry-function and
-bispectrum batches overlap on the device.  Results are copied to a pinned
+batch; the lanes' batches run in launch order on one compute stream (or on
+a stream per lane with ``overlap_lanes``), while uploads and copy-backs run on
+each lane's copy streams beside them.  Results are copied to a pinned
 host output ring per batch; a request completes when its batch's copy-back
 has finished, and its device ring space is freed when it is retired.
 
@@ -426,7 +427,7 @@ class ServingEngine:
     def __init__(self, lanes: dict, budget_bytes: int = 40 << 30, shares: dict | None = None,
                  max_batch_rows: int = 1 << 19, depth: int = 2, stage_bytes: int = 512 << 20,
                  out_rows: int | None = None, device=None, tuning: dict | None = None,
-                 pack_threads: int | None = None):
+                 pack_threads: int | None = None, overlap_lanes: bool = False):
         import concurrent.futures
         import os
 
@@ -448,6 +449,17 @@ class ServingEngine:
         out_rows = out_rows or 2 * max_batch_rows
         self.lanes = {k: _Lane(torch, k, v, caps[k], max_batch_rows, min(out_rows, caps[k].rows), stage_bytes, dev)
                       for k, v in lanes.items()}
+        # overlap_lanes: each lane's kernels on its own stream, so batches of
+        # different lanes share the SMs; otherwise one compute stream runs the
+        # lanes' batches in launch order (their copies still overlap them).  A
+        # bispectrum Z CTA needs a whole SM's shared memory and waits while
+        # symmetry-function CTAs hold part of one: on the B200 overlapped
+        # lanes ran no faster than lanes in turn, and up to 6% slower
+        self.overlap_lanes = bool(overlap_lanes)
+        if not self.overlap_lanes:
+            shared = torch.cuda.Stream(dev)
+            for ln in self.lanes.values():
+                ln.s_comp = shared
         for k, v in lanes.items():
             if tuning and k in tuning:
                 B.set_tuning(v, tuning[k])
