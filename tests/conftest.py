@@ -20,6 +20,29 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200)")
 
 
+def session_fill():
+    """LDB200_FILL_SCRATCH=<byte> (e.g. 0xff): the byte every device allocation
+    of the library is filled with for the whole session, or -1."""
+    v = os.environ.get("LDB200_FILL_SCRATCH")
+    return -1 if v is None else int(v, 0)
+
+
+@pytest.fixture(scope="session", autouse=True)
+def _session_scratch_fill():
+    """With LDB200_FILL_SCRATCH set, every test runs with the library's new
+    device allocations filled with that byte (0xff: NaN doubles), so that a
+    result depending on memory no kernel wrote fails its parity check."""
+    fill = session_fill()
+    if fill < 0:
+        yield
+        return
+    from abi import Abi
+
+    Abi.check(Abi.lib().ld_debug_fill_scratch(fill))
+    yield
+    Abi.lib().ld_debug_fill_scratch(-1)
+
+
 @pytest.fixture(scope="session")
 def oracle_mod():
     import oracle

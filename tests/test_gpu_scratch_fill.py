@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 from abi import Abi
-from conftest import golden_names, load_golden
+from conftest import golden_names, load_golden, session_fill
 from helpers import DESC_RTOL, GRAD_RTOL, assert_close, gpu_for, oracle_for
 
 pytestmark = pytest.mark.gpu
@@ -25,7 +25,7 @@ def filled_scratch():
     try:
         yield
     finally:
-        Abi.check(L.ld_debug_fill_scratch(-1))
+        Abi.check(L.ld_debug_fill_scratch(session_fill()))
 
 
 @pytest.mark.parametrize("name", golden_names())
