@@ -353,6 +353,9 @@ static int build_sf(ld_descriptor *d, int ns, const double *cutoff, int n_types,
     s.n3 = (int)o3.size();
     Arena ar;
     ar.add(rcut, &s.rcut);
+    std::vector<double> ircut(rcut.size());
+    for (size_t k = 0; k < rcut.size(); ++k) ircut[k] = rcut[k] > 0.0 ? 1.0 / rcut[k] : 0.0;
+    ar.add(ircut, &s.ircut);
     ar.add(o2, &s.o2);
     ar.add(t2, &s.t2);
     ar.add(a2, &s.a2);

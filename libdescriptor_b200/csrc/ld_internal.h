@@ -90,6 +90,7 @@ struct SFDev {
     int ns = 0, width = 0;
     int n2 = 0, n3 = 0;
     const double *rcut = nullptr;   // ns*ns
+    const double *ircut = nullptr;  // ns*ns, 1 / rcut
     const int *o2 = nullptr;        // output index
     const int *t2 = nullptr;        // 1..3
     const double *a2 = nullptr;     // eta (g2) / kappa (g3)

@@ -87,7 +87,7 @@ sf_kernel(SFDev p, RowArgs a, int per_warp_doubles, int *queue) {
             const double rx = x - cix, ry = y - ciy, rz = z - ciz;
             const double rsq = rx * rx + ry * ry + rz * rz;
             const double r = sqrt(rsq);
-            const double rc = p.rcut[is * p.ns + js];
+            const double rc = p.rcut[is * p.ns + js], irc = p.ircut[is * p.ns + js];
             S.cx[jj] = x;
             S.cy[jj] = y;
             S.cz[jj] = z;
@@ -97,12 +97,16 @@ sf_kernel(SFDev p, RowArgs a, int per_warp_doubles, int *queue) {
             S.spec[jj] = js;
             S.idx[jj] = ok ? j : -1;
             S.inc[jj] = ok && !(r > rc);
-            S.fc[jj] = cutc(r, rc);
             if (VJP) {
-                S.dfc[jj] = dcutc(r, rc);
+                double fc, dfc;
+                cutc_both(r, rc, irc, fc, dfc);
+                S.fc[jj] = fc;
+                S.dfc[jj] = dfc;
                 S.gx[jj] = 0.0;
                 S.gy[jj] = 0.0;
                 S.gz[jj] = 0.0;
+            } else {
+                S.fc[jj] = cutc_i(r, rc, irc);
             }
         }
         __syncwarp();
@@ -185,7 +189,7 @@ sf_kernel(SFDev p, RowArgs a, int per_warp_doubles, int *queue) {
                     // (same coordinates, same species-pair cutoff as the reference's
                     // per-triplet recomputation)
                     const int ks = S.spec[kk], js = S.spec[jj];
-                    const double rcjk = p.rcut[js * p.ns + ks];
+                    const double rcjk = p.rcut[js * p.ns + ks], ircjk = p.ircut[js * p.ns + ks];
                     const double jkx = S.cx[kk] - S.cx[jj], jky = S.cy[kk] - S.cy[jj], jkz = S.cz[kk] - S.cz[jj];
                     const double rjksq = jkx * jkx + jky * jky + jkz * jkz;
                     const double d = sqrt(rjksq);
@@ -195,17 +199,10 @@ sf_kernel(SFDev p, RowArgs a, int per_warp_doubles, int *queue) {
                     const double cth = (asq + bsq - dsq) * (0.5 * ia * ib);
                     const double fa = S.fc[jj], fb = S.fc[kk];
                     double fd = 0.0, dfd = 0.0;
-                    if (d < rcjk) {
-                        const double t = kPi * d / rcjk;
-                        if (VJP) {
-                            double sn, cs;
-                            sincos(t, &sn, &cs);
-                            fd = 0.5 * (cs + 1.0);
-                            dfd = -0.5 * sn * (kPi / rcjk);
-                        } else {
-                            fd = 0.5 * (cos(t) + 1.0);
-                        }
-                    }
+                    if (VJP)
+                        cutc_both(d, rcjk, ircjk, fd, dfd);
+                    else
+                        fd = cutc_i(d, rcjk, ircjk);
                     const bool g4ok = !(d > rcjk);
                     const double S4 = asq + bsq + dsq, S5 = asq + bsq;
                     const double F4 = fa * fb * fd, F5 = fa * fb;

@@ -23,6 +23,22 @@ __device__ __forceinline__ double cutc(double r, double rc) {
 __device__ __forceinline__ double dcutc(double r, double rc) {
     return (r < rc) ? -0.5 * sin(kPi * r / rc) * (kPi / rc) : 0.0;
 }
+// the cosine cutoff and its derivative from r / rc = r * irc (irc = 1 / rc):
+// one sincospi, no division, no reduction by pi
+__device__ __forceinline__ double cutc_i(double r, double rc, double irc) {
+    return (r < rc) ? 0.5 * (cospi(r * irc) + 1.0) : 0.0;
+}
+__device__ __forceinline__ void cutc_both(double r, double rc, double irc, double &fc, double &dfc) {
+    if (r < rc) {
+        double sn, cs;
+        sincospi(r * irc, &sn, &cs);
+        fc = 0.5 * (cs + 1.0);
+        dfc = -0.5 * sn * (kPi * irc);
+    } else {
+        fc = 0.0;
+        dfc = 0.0;
+    }
+}
 __device__ __forceinline__ double ipow(double x, int n) {
     double r = 1.0;
     for (int k = 0; k < n; ++k) r *= x;

@@ -110,7 +110,7 @@ sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue)
             const double x = a.coords[3 * j], y = a.coords[3 * j + 1], z = a.coords[3 * j + 2];
             const double rx = x - cix, ry = y - ciy, rz = z - ciz;
             const double r = sqrt(rx * rx + ry * ry + rz * rz);
-            const double rc = p.rcut[is * p.ns + js];
+            const double rc = p.rcut[is * p.ns + js], irc = p.ircut[is * p.ns + js];
             S.cx[jj] = x;
             S.cy[jj] = y;
             S.cz[jj] = z;
@@ -120,12 +120,16 @@ sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue)
             S.spec[jj] = js;
             S.idx[jj] = ok ? j : -1;
             S.inc[jj] = ok && !(r > rc);
-            S.fc[jj] = cutc(r, rc);
             if (VJP) {
-                S.dfc[jj] = dcutc(r, rc);
+                double fc, dfc;
+                cutc_both(r, rc, irc, fc, dfc);
+                S.fc[jj] = fc;
+                S.dfc[jj] = dfc;
                 S.gx[jj] = 0.0;
                 S.gy[jj] = 0.0;
                 S.gz[jj] = 0.0;
+            } else {
+                S.fc[jj] = cutc_i(r, rc, irc);
             }
         }
         __syncwarp();
@@ -242,7 +246,7 @@ sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue)
                 if (kk >= n) kk -= n;
                 if (incj && (dd <= dmax || jj < dlast) && S.inc[kk]) {
                     const int ks = S.spec[kk];
-                    const double rcjk = p.rcut[js * p.ns + ks];
+                    const double rcjk = p.rcut[js * p.ns + ks], ircjk = p.ircut[js * p.ns + ks];
                     const double jkx = S.cx[kk] - cxj, jky = S.cy[kk] - cyj, jkz = S.cz[kk] - czj;
                     const double d = sqrt(jkx * jkx + jky * jky + jkz * jkz);
                     const double b = S.r[kk];
@@ -251,16 +255,11 @@ sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue)
                     const double cth = (asq + bsq - dsq) * (0.5 * ia * ib);
                     const double fb = S.fc[kk];
                     double fd = 0.0, dfd = 0.0;
-                    if (HAS4 && d < rcjk) {
-                        const double t = kPi * d / rcjk;
-                        if (VJP) {
-                            double sn, cs;
-                            sincos(t, &sn, &cs);
-                            fd = 0.5 * (cs + 1.0);
-                            dfd = -0.5 * sn * (kPi / rcjk);
-                        } else {
-                            fd = 0.5 * (cos(t) + 1.0);
-                        }
+                    if (HAS4) {
+                        if (VJP)
+                            cutc_both(d, rcjk, ircjk, fd, dfd);
+                        else
+                            fd = cutc_i(d, rcjk, ircjk);
                     }
                     const bool g4ok = !(d > rcjk);
                     double Aq[NT] = {0.0, 0.0}, Bq[NT] = {0.0, 0.0}, Cq[NT] = {0.0, 0.0};
