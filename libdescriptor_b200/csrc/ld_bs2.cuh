@@ -55,9 +55,26 @@ __device__ __forceinline__ double sfac_of(const BSDev &p, double r, double rc) {
     if (p.switch_flag == 1) {
         if (r <= p.rmin0) return 1.0;
         if (r > rc) return 0.0;
-        return 0.5 * (cos((r - p.rmin0) * kPi / (rc - p.rmin0)) + 1.0);
+        return 0.5 * (cospi((r - p.rmin0) / (rc - p.rmin0)) + 1.0);
     }
     return 0.0;
+}
+// the switching function and its derivative together (one division, one
+// sincospi of (r - rmin0) / (rc - rmin0))
+__device__ __forceinline__ void sfac_both(const BSDev &p, double r, double rc, double &sf, double &dsf) {
+    sf = p.switch_flag == 0 ? 1.0 : 0.0;
+    dsf = 0.0;
+    if (p.switch_flag == 1) {
+        if (r <= p.rmin0) {
+            sf = 1.0;
+        } else if (!(r > rc)) {
+            const double inv = 1.0 / (rc - p.rmin0);
+            double sn, cs;
+            sincospi((r - p.rmin0) * inv, &sn, &cs);
+            sf = 0.5 * (cs + 1.0);
+            dsf = -0.5 * sn * (kPi * inv);
+        }
+    }
 }
 __device__ __forceinline__ double dsfac_of(const BSDev &p, double r, double rc) {
     if (p.switch_flag == 1) {
@@ -78,18 +95,21 @@ struct CK {
 template <bool TAN>
 __device__ __forceinline__ void cayley_klein(const BSDev &p, double x, double y, double z, double r, double rc,
                                              CK &c) {
-    const double theta0 = (r - p.rmin0) * p.rfac0 * kPi / (rc - p.rmin0);
-    const double z0 = r / tan(theta0);
-    const double r0inv = 1.0 / sqrt(r * r + z0 * z0);
+    // theta0 = (r - rmin0) c0, z0 = r / tan(theta0) = r cos / sin: one
+    // sincos and one reciprocal serve the parameters and their tangents
+    const double c0 = p.rfac0 * kPi / (rc - p.rmin0);
+    const double theta0 = (r - p.rmin0) * c0;
+    double sth, cth;
+    sincos(theta0, &sth, &cth);
+    const double isth = 1.0 / sth;
+    const double z0 = r * cth * isth;
+    const double r0inv = rsqrt(r * r + z0 * z0);
     c.ar = r0inv * z0;
     c.ai = -r0inv * z;
     c.br = r0inv * y;
     c.bi = -r0inv * x;
     if (TAN) {
-        const double c0 = p.rfac0 * kPi / (rc - p.rmin0);
-        double sth, cth;
-        sincos(theta0, &sth, &cth);
-        const double dz0 = cth / sth - r * c0 / (sth * sth);
+        const double dz0 = cth * isth - r * c0 * isth * isth;
         const double dr0inv = -r0inv * r0inv * r0inv * (r + z0 * dz0);
         const double rinv = 1.0 / r;
         const double u3[3] = {x * rinv, y * rinv, z * rinv};
