@@ -287,7 +287,7 @@ sf_kernel(SFDev p, RowArgs a, int per_warp_doubles, int *queue) {
                                           F5 * C5 * dcb - 2.0 * b * F5 * B5 + fa * dfb * A5;
                         const double Gd = F4 * C4 * dcd - 2.0 * d * F4 * B4 + fa * fb * dfd * A4 +
                                           F5 * C5 * dcd;
-                        const double id = d > 0 ? 1.0 / d : 0.0;
+                        const double id = d > 0 ? rsqrt(dsq) : 0.0;
                         const double ijx = (S.cx[jj] - cix) * ia, ijy = (S.cy[jj] - ciy) * ia,
                                      ijz = (S.cz[jj] - ciz) * ia;
                         const double ukx = (S.cx[kk] - cix) * ib, uky = (S.cy[kk] - ciy) * ib,

@@ -369,7 +369,7 @@ sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue)
                         const double Gb = F4 * C4 * dcb - 2.0 * b * F4 * B4 + fa * dfb * fd * A4 +
                                           F5 * C5 * dcb - 2.0 * b * F5 * B5 + fa * dfb * A5;
                         const double Gd = F4 * C4 * dcd - 2.0 * d * F4 * B4 + fa * fb * dfd * A4 + F5 * C5 * dcd;
-                        const double id = d > 0 ? 1.0 / d : 0.0;
+                        const double id = d > 0 ? rsqrt(dsq) : 0.0;
                         const double ijx = (cxj - cix) * ia, ijy = (cyj - ciy) * ia, ijz = (czj - ciz) * ia;
                         const double ukx = (S.cx[kk] - cix) * ib, uky = (S.cy[kk] - ciy) * ib,
                                      ukz = (S.cz[kk] - ciz) * ib;
