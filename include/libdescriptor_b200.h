@@ -289,6 +289,26 @@ int ld_stage_upload(int n_atoms, int n_total, long long nnz, int width,
                     int *d_centre, long long *d_begin, int *d_counts, double *d_dE,
                     ld_stream stream);
 
+/* Staging by chunk (no reference counterpart): requests admitted together
+ * into consecutive ring slots share one staging block laid out field by field
+ * (all their coordinates, then all species, ... in admission order), so the
+ * block uploads with one copy per field instead of one per field and request.
+ * ld_stage_pack_fields writes one request's fields at the given host pointers
+ * -- the request's place inside each field's run -- with indices rebased to
+ * the slots and checked exactly as ld_stage_pack does; it touches no device
+ * and calls for different requests may run concurrently.
+ * ld_stage_upload_fields enqueues n_fields host-to-device copies
+ * (dst[i] <- src[i], bytes[i]; zero-byte entries are skipped) on `stream`. */
+int ld_stage_pack_fields(int n_atoms, int n_total, long long nnz, int width,
+                         int row0, int atom0, long long entry0,
+                         const double *coords, const int *species, const int *image,
+                         const int *neighbor_list, const int *number_of_neighs,
+                         const double *dE_ddesc, double *coords_out, int *species_out,
+                         int *image_out, int *nbl_out, int *centre_out, long long *begin_out,
+                         int *counts_out, double *dE_out);
+int ld_stage_upload_fields(int n_fields, const void *const *src, void *const *dst,
+                           const size_t *bytes, ld_stream stream);
+
 /* Descriptor + VJP pass that allocates no device memory (no counterpart in
  * the reference; it serves callers that cannot call cudaMalloc while they
  * evaluate forces, e.g. engines whose device memory is owned by their own

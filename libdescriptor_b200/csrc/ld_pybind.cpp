@@ -437,6 +437,35 @@ PYBIND11_MODULE(_libdescriptor, m) {
         }
         check(rc);
     });
+    m.def("_stage_pack_fields", [](int n, int nt, long long nnz, int width, int row0, int atom0, long long entry0,
+                                   DArr coords, IArr species, IArr image, IArr nbl, IArr counts, DArr dE,
+                                   std::vector<std::uintptr_t> out) {
+        if ((long long)coords.size() < 3LL * nt || (long long)species.size() < nt || (long long)image.size() < nt ||
+            (long long)nbl.size() < nnz || (long long)counts.size() < n || (long long)dE.size() < (long long)n * width)
+            throw py::value_error("_stage_pack_fields: arrays shorter than the stated sizes");
+        if (out.size() != 8) throw py::value_error("_stage_pack_fields: 8 output fields");
+        int rc;
+        {
+            py::gil_scoped_release nogil;
+            rc = ld_stage_pack_fields(n, nt, nnz, width, row0, atom0, entry0, coords.data(), species.data(),
+                                      image.data(), nnz ? nbl.data() : nullptr, counts.data(), dE.data(),
+                                      (double *)out[0], (int *)out[1], (int *)out[2], (int *)out[3], (int *)out[4],
+                                      (long long *)out[5], (int *)out[6], (double *)out[7]);
+        }
+        check(rc);
+    });
+    m.def("_stage_upload_fields", [](std::vector<std::uintptr_t> src, std::vector<std::uintptr_t> dst,
+                                     std::vector<std::size_t> bytes, std::uintptr_t stream) {
+        if (src.size() != dst.size() || src.size() != bytes.size())
+            throw py::value_error("_stage_upload_fields: src, dst and bytes differ in length");
+        std::vector<const void *> s(src.size());
+        std::vector<void *> d(dst.size());
+        for (size_t i = 0; i < src.size(); ++i) {
+            s[i] = (const void *)src[i];
+            d[i] = (void *)dst[i];
+        }
+        check(ld_stage_upload_fields((int)src.size(), s.data(), d.data(), bytes.data(), (ld_stream)stream));
+    });
     m.def("_stage_upload", [](int n, int nt, long long nnz, int width, int row0, int atom0, long long entry0,
                               std::uintptr_t staging, std::size_t staging_bytes, std::uintptr_t d_coords,
                               std::uintptr_t d_species, std::uintptr_t d_image, std::uintptr_t d_nbl,

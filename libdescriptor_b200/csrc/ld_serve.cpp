@@ -8,6 +8,10 @@
 // every index rebased to those slots, into pinned staging memory and
 // enqueues one upload per field on the given stream: after it the rows can
 // join any batch launched through ld_gradient_rows_dev on the rings.
+// ld_stage_pack_fields / ld_stage_upload_fields do the same for requests
+// admitted together into consecutive slots: each request's fields go to its
+// place in one block laid out field by field, uploaded with one copy per
+// field for the whole block.
 #include <cstdint>
 #include <cstring>
 #include <string>
@@ -80,9 +84,12 @@ int check_staging(void *staging, size_t staging_bytes, const StageLayout &L, con
     return LD_OK;
 }
 
+int stage_pack_fields(int n_atoms, int n_total, long long nnz, int width, int row0, int atom0, long long entry0,
+                      const double *coords, const int *species, const int *image, const int *neighbor_list,
+                      const int *number_of_neighs, const double *dE_ddesc, const Fields &F, int max_threads);
+
 // The host half of staging: every field of the request into the staging
-// layout, indices rebased and range-checked.  max_threads 0: one host
-// thread per MiB of copying, up to the cores (at most 16); 1: this thread.
+// layout (see stage_pack_fields).
 int stage_pack(int n_atoms, int n_total, long long nnz, int width, int row0, int atom0, long long entry0,
                const double *coords, const int *species, const int *image, const int *neighbor_list,
                const int *number_of_neighs, const double *dE_ddesc, void *staging, size_t staging_bytes,
@@ -94,8 +101,17 @@ int stage_pack(int n_atoms, int n_total, long long nnz, int width, int row0, int
         return fail(LD_ERR_INVALID_ARG, std::string(who) + ": NULL array");
     const StageLayout L = layout(n_atoms, n_total, nnz, width);
     if (int rc = check_staging(staging, staging_bytes, L, who)) return rc;
-    const Fields F = fields(staging, L);
+    return stage_pack_fields(n_atoms, n_total, nnz, width, row0, atom0, entry0, coords, species, image,
+                             neighbor_list, number_of_neighs, dE_ddesc, fields(staging, L), max_threads);
+}
 
+// Every field of one request written at the given host pointers, indices
+// rebased to the slots and range-checked.  max_threads 0: one host thread
+// per MiB of copying, up to the cores (at most 16); 1: this thread.
+int stage_pack_fields(int n_atoms, int n_total, long long nnz, int width, int row0, int atom0, long long entry0,
+                      const double *coords, const int *species, const int *image, const int *neighbor_list,
+                      const int *number_of_neighs, const double *dE_ddesc, const Fields &F, int max_threads) {
+    using namespace ldb;
     // row arrays (sequential prefix) + count check
     long long pos = entry0;
     for (int j = 0; j < n_atoms; ++j) {
@@ -215,6 +231,38 @@ extern "C" int ld_stage_pack(int n_atoms, int n_total, long long nnz, int width,
                              void *staging, size_t staging_bytes) {
     return stage_pack(n_atoms, n_total, nnz, width, row0, atom0, entry0, coords, species, image, neighbor_list,
                       number_of_neighs, dE_ddesc, staging, staging_bytes, 1, "ld_stage_pack");
+}
+
+extern "C" int ld_stage_pack_fields(int n_atoms, int n_total, long long nnz, int width, int row0, int atom0,
+                                    long long entry0, const double *coords, const int *species, const int *image,
+                                    const int *neighbor_list, const int *number_of_neighs, const double *dE_ddesc,
+                                    double *coords_out, int *species_out, int *image_out, int *nbl_out,
+                                    int *centre_out, long long *begin_out, int *counts_out, double *dE_out) {
+    using namespace ldb;
+    if (n_atoms <= 0 || n_total < n_atoms || nnz < 0 || width <= 0 || row0 < 0 || atom0 < 0 || entry0 < 0)
+        return fail(LD_ERR_INVALID_ARG, "ld_stage_pack_fields: bad sizes or slots");
+    if (!coords || !species || !image || !number_of_neighs || !dE_ddesc || (nnz > 0 && !neighbor_list))
+        return fail(LD_ERR_INVALID_ARG, "ld_stage_pack_fields: NULL array");
+    if (!coords_out || !species_out || !image_out || (nnz > 0 && !nbl_out) || !centre_out || !begin_out ||
+        !counts_out || !dE_out)
+        return fail(LD_ERR_INVALID_ARG, "ld_stage_pack_fields: NULL output field");
+    const Fields F{coords_out, species_out, image_out, nbl_out, centre_out, begin_out, counts_out, dE_out};
+    return stage_pack_fields(n_atoms, n_total, nnz, width, row0, atom0, entry0, coords, species, image,
+                             neighbor_list, number_of_neighs, dE_ddesc, F, 1);
+}
+
+extern "C" int ld_stage_upload_fields(int n_fields, const void *const *src, void *const *dst, const size_t *bytes,
+                                      ld_stream stream) {
+    using namespace ldb;
+    if (n_fields < 0 || n_fields > 64 || (n_fields > 0 && (!src || !dst || !bytes)))
+        return fail(LD_ERR_INVALID_ARG, "ld_stage_upload_fields: bad field list");
+    for (int i = 0; i < n_fields; ++i)
+        if (bytes[i] > 0 && (!src[i] || !dst[i]))
+            return fail(LD_ERR_INVALID_ARG, "ld_stage_upload_fields: NULL field pointer");
+    cudaStream_t s = (cudaStream_t)stream;
+    for (int i = 0; i < n_fields; ++i)
+        if (bytes[i] > 0) LDB_CUDA(cudaMemcpyAsync(dst[i], src[i], bytes[i], cudaMemcpyHostToDevice, s));
+    return LD_OK;
 }
 
 extern "C" int ld_stage_upload(int n_atoms, int n_total, long long nnz, int width, int row0, int atom0,

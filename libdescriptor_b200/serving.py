@@ -381,6 +381,63 @@ class Scheduler:
         return done
 
 
+# ------------------------------------------------------------ staging plan
+# per staged field: bytes per atom (coords, species, image), per entry (nbl)
+# or per row (centre, begin, counts; dE takes 8 * width)
+_FIELD_UNITS = (("atom", 24), ("atom", 4), ("atom", 4), ("entry", 4), ("row", 4), ("row", 8), ("row", 4),
+                ("row", None))
+
+
+def field_bytes(n: int, nt: int, nnz: int, width: int) -> list:
+    """Bytes of each staged field of one request (ld_stage_pack's order)."""
+    per = {"atom": nt, "entry": nnz, "row": n}
+    return [per[k] * (8 * width if b is None else b) for k, b in _FIELD_UNITS]
+
+
+def stage_chunks(items: list, cap_bytes: int) -> list:
+    """Split requests (in admission order) into staging chunks.
+
+    items: (n_atoms, n_total, nnz, width, (row0, atom0, entry0)) per request.
+    A chunk is a run of requests whose ring slots continue one another in
+    all three rings (no wrap in between), so that each field of the run is
+    one contiguous device range; a chunk is closed before it would exceed
+    cap_bytes of staging (a larger request stands alone).  Returns lists of
+    indices into items."""
+    chunks, cur, nxt, size = [], [], None, 0
+    for i, (n, nt, nnz, w, slots) in enumerate(items):
+        b = sum(field_bytes(n, nt, nnz, w))
+        if cur and tuple(slots) == nxt and size + b <= cap_bytes:
+            cur.append(i)
+            size += b
+        else:
+            if cur:
+                chunks.append(cur)
+            cur, size = [i], b
+        nxt = (slots[0] + n, slots[1] + nt, slots[2] + nnz)
+    if cur:
+        chunks.append(cur)
+    return chunks
+
+
+def chunk_layout(items: list, align: int = 256):
+    """Field-by-field layout of one chunk's staging block.
+
+    Returns (starts, totals, offsets, block_bytes): the byte offset of each
+    field's run in the block (aligned), each run's length, and per request
+    the byte offset of its part inside each run."""
+    sizes = [field_bytes(n, nt, nnz, w) for n, nt, nnz, w, _ in items]
+    totals = [sum(col) for col in zip(*sizes)] if sizes else [0] * len(_FIELD_UNITS)
+    starts, t = [], 0
+    for tot in totals:
+        starts.append(t)
+        t += (tot + align - 1) // align * align
+    offsets, run = [], [0] * len(totals)
+    for sz in sizes:
+        offsets.append(list(run))
+        run = [a + b for a, b in zip(run, sz)]
+    return starts, totals, offsets, t
+
+
 # ------------------------------------------------------------ device side
 class _Lane:
     """Device rings, pinned staging and streams of one descriptor kind."""
@@ -498,9 +555,10 @@ class ServingEngine:
             ln.stage_ring.free(u0)
 
     def stage(self, req: Request) -> None:
-        """Reserve pinned staging for one admitted request; ``flush`` packs it
-        (``ld_stage_pack``, native, indices rebased) and uploads it
-        (``ld_stage_upload``)."""
+        """Queue one admitted request for staging; ``flush`` packs the
+        admitted requests into pinned staging chunk by chunk
+        (``ld_stage_pack_fields``, native, indices rebased) and uploads each
+        chunk with one copy per field (``ld_stage_upload_fields``)."""
         torch = self.torch
         torch.cuda.nvtx.range_push(f"serve: stage request {req.rid}")
         try:
@@ -509,72 +567,91 @@ class ServingEngine:
             torch.cuda.nvtx.range_pop()
 
     def _stage(self, req: Request) -> None:
-        """Reserve the request's pinned staging space; the packing and the
-        uploads follow in ``flush`` (packing on host threads, uploads in
-        admission order)."""
-        ln = self.lanes[req.lane]
-        n, nt, nnz, W = req.n_atoms, req.n_total, req.nnz, ln.W
-        t_in = time.perf_counter()
-        nbytes = int(self._ext._stage_bytes(n, nt, nnz, W))
-        units = max((nbytes + 255) // 256, 1)
-        self._reclaim_staging(ln)
-        u0 = ln.stage_ring.alloc(units)
-        while u0 is None:
-            # staging full: upload what is packed, then wait for the oldest upload
-            if any(job[1] is ln for job in self._jobs):
-                self.flush()
-            if not ln.staged:
-                raise RuntimeError("request larger than the pinned staging ring")
-            ln.staged[0][1].synchronize()
-            self._reclaim_staging(ln)
-            u0 = ln.stage_ring.alloc(units)
-        self._jobs.append((req, ln, u0, units, nbytes))
-        self.host_stage_s += time.perf_counter() - t_in
+        self._jobs.append((req, self.lanes[req.lane]))
 
     def _pack(self, job) -> None:
-        req, ln, u0, units, _ = job
+        req, outs = job
         r0, a0, e0 = req.slots
-        self._ext._stage_pack(req.n_atoms, req.n_total, req.nnz, ln.W, r0, a0, e0, req.coords, req.species,
-                              req.image, req.nbl, req.counts, req.dE, ln.stage.data_ptr() + 256 * u0, units * 256)
+        self._ext._stage_pack_fields(req.n_atoms, req.n_total, req.nnz, self.lanes[req.lane].W, r0, a0, e0,
+                                     req.coords, req.species, req.image, req.nbl, req.counts, req.dE, outs)
 
     def _pack_group(self, jobs) -> None:
         for job in jobs:
             self._pack(job)
 
     def flush(self) -> None:
-        """Pack the reserved requests into pinned staging, spread over host
-        threads when there is enough to copy, then enqueue their uploads and
-        mark each with an event, in admission order."""
+        """Stage the queued requests: per lane, runs of requests in
+        consecutive ring slots form chunks (``stage_chunks``); each chunk
+        gets one pinned staging block laid out field by field, its requests
+        are packed into it (on host threads when there is enough to copy),
+        and it is uploaded with one copy per field, marked by one event."""
         if not self._jobs:
             return
-        torch = self.torch
         t_in = time.perf_counter()
         jobs, self._jobs = self._jobs, []
-        total = sum(j[4] for j in jobs)
+        by_lane: dict = {}
+        for req, ln in jobs:
+            by_lane.setdefault(ln.name, (ln, []))[1].append(req)
+        for ln, reqs in by_lane.values():
+            cap = max(1 << 20, ln.stage.numel() // 4)
+            items = [(r.n_atoms, r.n_total, r.nnz, ln.W, r.slots) for r in reqs]
+            pending = []
+            for ch in stage_chunks(items, cap):
+                lay = chunk_layout([items[i] for i in ch])
+                units = max((lay[3] + 255) // 256, 1)
+                self._reclaim_staging(ln)
+                u0 = ln.stage_ring.alloc(units)
+                while u0 is None:
+                    # staging full: pack and upload what is reserved, else
+                    # wait for the oldest upload to free its block
+                    if pending:
+                        self._pack_upload(ln, pending)
+                        pending = []
+                    elif not ln.staged:
+                        raise RuntimeError("request larger than the pinned staging ring")
+                    else:
+                        ln.staged[0][1].synchronize()
+                    self._reclaim_staging(ln)
+                    u0 = ln.stage_ring.alloc(units)
+                pending.append(([reqs[i] for i in ch], u0, lay))
+            if pending:
+                self._pack_upload(ln, pending)
+        self.host_stage_s += time.perf_counter() - t_in
+
+    def _pack_upload(self, ln: _Lane, chunks: list) -> None:
+        torch = self.torch
+        base = ln.stage.data_ptr()
+        jobs, total = [], 0
+        for reqs, u0, (starts, totals, offsets, nbytes) in chunks:
+            blk = base + 256 * u0
+            for req, off in zip(reqs, offsets):
+                jobs.append((req, [blk + st + o for st, o in zip(starts, off)]))
+            total += nbytes
         if self._pool is None or len(jobs) == 1 or total < (4 << 20):
             self._pack_group(jobs)
         else:
             # longest first onto the least loaded of the workers
             groups = [[] for _ in range(min(self._pack_threads, len(jobs)))]
             load = [0] * len(groups)
-            for job in sorted(jobs, key=lambda j: -j[4]):
+            for job in sorted(jobs, key=lambda j: -(j[0].n_total + j[0].nnz + j[0].n_atoms * ln.W)):
                 g = load.index(min(load))
                 groups[g].append(job)
-                load[g] += job[4]
+                load[g] += job[0].n_total + job[0].nnz + job[0].n_atoms * ln.W
             for f in [self._pool.submit(self._pack_group, g) for g in groups]:
                 f.result()
-        for req, ln, u0, units, _ in jobs:
-            r0, a0, e0 = req.slots
-            self._ext._stage_upload(req.n_atoms, req.n_total, req.nnz, ln.W, r0, a0, e0,
-                                    ln.stage.data_ptr() + 256 * u0, units * 256, ln.coords.data_ptr(),
-                                    ln.species.data_ptr(), ln.image.data_ptr(), ln.nbl.data_ptr(),
-                                    ln.centre.data_ptr(), ln.begin.data_ptr(), ln.counts.data_ptr(),
-                                    ln.dE.data_ptr(), ln.s_h2d.cuda_stream)
+        W = ln.W
+        for reqs, u0, (starts, totals, offsets, nbytes) in chunks:
+            r0, a0, e0 = reqs[0].slots
+            blk = base + 256 * u0
+            dst = [ln.coords.data_ptr() + 24 * a0, ln.species.data_ptr() + 4 * a0, ln.image.data_ptr() + 4 * a0,
+                   ln.nbl.data_ptr() + 4 * e0, ln.centre.data_ptr() + 4 * r0, ln.begin.data_ptr() + 8 * r0,
+                   ln.counts.data_ptr() + 4 * r0, ln.dE.data_ptr() + 8 * W * r0]
+            self._ext._stage_upload_fields([blk + st for st in starts], dst, list(totals), ln.s_h2d.cuda_stream)
             ev = torch.cuda.Event()
             ev.record(ln.s_h2d)
             ln.staged.append((u0, ev))
-            req.staged = ev
-        self.host_stage_s += time.perf_counter() - t_in
+            for req in reqs:
+                req.staged = ev
 
     def launch(self, plan: BatchPlan) -> None:
         torch = self.torch

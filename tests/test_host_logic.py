@@ -364,6 +364,87 @@ def test_stage_pack_writes_what_stage_request_writes():
                            np.asarray(counts, np.int32), dE.ravel(), C.c_void_p(base), nb.value) == 2
 
 
+def test_stage_chunks_follow_ring_contiguity_and_cap():
+    """Requests in consecutive slots of all three rings share a chunk; a wrap
+    (or any gap) in one ring, or the byte cap, starts a new one."""
+    from libdescriptor_b200.serving import field_bytes, stage_chunks
+
+    W = 4
+    items = [(3, 5, 6, W, (0, 0, 0)), (2, 4, 3, W, (3, 5, 6)), (1, 1, 0, W, (5, 9, 9)),
+             (2, 2, 2, W, (0, 10, 9)),            # row ring wrapped
+             (2, 3, 1, W, (2, 12, 11)),
+             (4, 4, 4, W, (4, 16, 12))]           # atom gap (16 != 15)
+    assert stage_chunks(items, 1 << 30) == [[0, 1, 2], [3, 4], [5]]
+    b0 = sum(field_bytes(3, 5, 6, W))
+    assert stage_chunks(items[:3], b0) == [[0], [1, 2]]
+    assert stage_chunks([], 1 << 20) == []
+
+
+def test_chunk_pack_fields_equal_per_request_staging():
+    """Two requests in consecutive slots packed field by field into one chunk
+    (ld_stage_pack_fields through the module, no device) hold exactly the
+    fields ld_stage_pack writes for each request alone, in admission order."""
+    import ctypes as C
+
+    from abi import Abi
+    from libdescriptor_b200 import _ext
+    from libdescriptor_b200.serving import chunk_layout
+
+    W = 2
+    reqs = [dict(n=3, nt=5, counts=[2, 0, 3], nbl=[1, 4, 0, 2, 3], image=[0, 1, 2, 0, 2]),
+            dict(n=2, nt=3, counts=[1, 2], nbl=[2, 0, 1], image=[0, 1, 1])]
+    rng = np.random.default_rng(4)
+    slots, r0, a0, e0 = [], 7, 40, 300
+    for q in reqs:
+        q["coords"] = rng.normal(size=(q["nt"], 3))
+        q["species"] = (np.arange(q["nt"]) % 2).astype(np.int32)
+        q["dE"] = rng.normal(size=(q["n"], W))
+        slots.append((r0, a0, e0))
+        r0, a0, e0 = r0 + q["n"], a0 + q["nt"], e0 + len(q["nbl"])
+    items = [(q["n"], q["nt"], len(q["nbl"]), W, sl) for q, sl in zip(reqs, slots)]
+    starts, totals, offsets, nbytes = chunk_layout(items)
+    raw = np.zeros(nbytes + 512, np.uint8)
+    base = (raw.ctypes.data + 255) & ~255
+    for q, sl, off in zip(reqs, slots, offsets):
+        _ext._stage_pack_fields(q["n"], q["nt"], len(q["nbl"]), W, sl[0], sl[1], sl[2],
+                                np.ascontiguousarray(q["coords"]).ravel(), q["species"],
+                                np.asarray(q["image"], np.int32), np.asarray(q["nbl"], np.int32),
+                                np.asarray(q["counts"], np.int32), q["dE"].ravel(),
+                                [base + st + o for st, o in zip(starts, off)])
+    chunk = raw[base - raw.ctypes.data:][:nbytes]
+    # each request alone through ld_stage_pack, fields concatenated in order
+    L = Abi.lib()
+    want = [b"" for _ in range(8)]
+    for q, sl in zip(reqs, slots):
+        nb = C.c_size_t()
+        Abi.check(L.ld_stage_bytes(q["n"], q["nt"], len(q["nbl"]), W, C.byref(nb)))
+        r = np.zeros(nb.value + 512, np.uint8)
+        rb = (r.ctypes.data + 255) & ~255
+        Abi.check(L.ld_stage_pack(q["n"], q["nt"], len(q["nbl"]), W, sl[0], sl[1], sl[2],
+                                  np.ascontiguousarray(q["coords"]).ravel(), q["species"],
+                                  np.asarray(q["image"], np.int32), np.asarray(q["nbl"], np.int32),
+                                  np.asarray(q["counts"], np.int32), q["dE"].ravel(), C.c_void_p(rb), nb.value))
+        buf = r[rb - r.ctypes.data:]
+        sizes = [q["nt"] * 24, q["nt"] * 4, q["nt"] * 4, len(q["nbl"]) * 4, q["n"] * 4, q["n"] * 8, q["n"] * 4,
+                 q["n"] * W * 8]
+        off = 0
+        for f, sz in enumerate(sizes):
+            want[f] += buf[off:off + sz].tobytes()
+            off += (sz + 255) // 256 * 256
+    for f in range(8):
+        assert chunk[starts[f]:starts[f] + totals[f]].tobytes() == want[f], f"field {f}"
+
+
+def test_stage_upload_fields_checks_its_list():
+    from libdescriptor_b200 import _ext
+
+    with pytest.raises(ValueError):
+        _ext._stage_upload_fields([1, 2], [3], [8, 8], 0)
+    with pytest.raises((RuntimeError, ValueError)):
+        _ext._stage_upload_fields([0], [4096], [8], 0)      # NULL source with bytes to copy
+    _ext._stage_upload_fields([0], [0], [0], 0)             # nothing to copy: no device needed
+
+
 @pytest.mark.parametrize("bad", ["nbl", "image", "counts"])
 def test_stage_request_rejects_bad_indices(bad):
     from abi import Abi
