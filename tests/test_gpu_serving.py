@@ -67,3 +67,30 @@ def test_poisson_stream_matches_alone(stream_setup):
     st = eng.serve(reqs, S.poisson_arrivals(len(reqs), 4000.0, seed=9), keep_results=True)
     assert st["requests"] == 40 and st["p99_ms"] >= st["p50_ms"] > 0
     _check(reqs, alone)
+
+
+def test_style2_bispectrum_lane_with_nan_filled_work_space():
+    """A bispectrum lane whose odd layers hold no needed triples (style 2):
+    the served batches' work space (a torch buffer) filled with NaN bytes
+    before serving, every request's results still equal its plain call."""
+    import libdescriptor_b200 as lds
+    from libdescriptor_b200 import serving as S
+
+    kinds = {"bs": lds.DescriptorKind.init_descriptor(lds.AvailableDescriptors.Bispectrum, 0.99363, 4, 2, 0, 0.0, 1,
+                                                      0, 5.0, ["A", "B"], [1.0, 0.5])}
+    pool = S.packing_pool(6, n_min=16, n_max=400, seed=15)
+    widths = {k: int(v.width) for k, v in kinds.items()}
+    reqs = S.make_requests(pool, 16, widths, {"bs": 1.0}, seed=16)
+    alone = []
+    for r in reqs:
+        d, g = lds.compute_and_gradient(kinds["bs"], r.n_atoms, r.species, r.nbl, r.counts, r.coords, r.dE)
+        alone.append((d, S.fold_host(g, r.n_atoms, r.image)))
+    eng = S.ServingEngine(kinds, budget_bytes=64 << 20, max_batch_rows=2048, stage_bytes=8 << 20)
+    for ln in eng.lanes.values():
+        ln.work.fill_(0xFF)
+    import torch
+
+    torch.cuda.synchronize()
+    eng.serve(reqs, None, keep_results=True)
+    eng.close()
+    _check(reqs, alone)
