@@ -566,6 +566,11 @@ def run_serve(args, torch, lds, dev, world, rank, local, dist):
                           "served": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in sv.items()},
                           "plain": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in pl.items()},
                           "served_over_plain": sv["atoms_per_s"] / pl["atoms_per_s"]})
+        # whole-job end-to-end rates: every rank's atoms over the slowest
+        # rank's span (each rank serves its own stream)
+        top = max(RATES)
+        e2e_served, _, _ = replica_throughput(served[top]["atoms"], 1e3 * served[top]["seconds"], dist, dev)
+        e2e_plain, _, _ = replica_throughput(plain[top]["atoms"], 1e3 * plain[top]["seconds"], dist, dev)
     if rank != 0:
         return None
     top, low = max(RATES), min(RATES)
@@ -603,15 +608,15 @@ def run_serve(args, torch, lds, dev, world, rank, local, dist):
                     + r.dE.nbytes + 12 * r.n_atoms for r in reqs)
     d2h_bytes = sum(8 * r.n_atoms * (widths[r.lane] + 3) for r in reqs)
     atoms_total = sum(r.n_atoms for r in reqs)
-    e2e = {"value": world * served[top]["atoms_per_s"], "unit": "atoms/s",
+    e2e = {"value": e2e_served, "unit": "atoms/s",
            "h2d_bytes_per_step": int(h2d_bytes / n_steps_stream), "d2h_bytes_per_step": int(d2h_bytes / n_steps_stream),
            "api": "libdescriptor_b200.serving.ServingEngine.serve (host numpy requests in, host results out), "
                   f"{N_STREAM} requests, Poisson arrivals at {int(top)}/s",
            "p50_ms": served[top]["p50_ms"], "p99_ms": served[top]["p99_ms"],
-           "plain_call": {"value": world * plain[top]["atoms_per_s"], "p50_ms": plain[top]["p50_ms"],
+           "plain_call": {"value": e2e_plain, "p50_ms": plain[top]["p50_ms"],
                           "p99_ms": plain[top]["p99_ms"],
                           "api": "libdescriptor_b200.compute_and_gradient per request + host fold"},
-           "served_over_plain": served[top]["atoms_per_s"] / plain[top]["atoms_per_s"],
+           "served_over_plain": e2e_served / e2e_plain,
            "rate_sweep": sweep}
     cdesc = {"workload": "served_mixed_stream_sf24_70_bs2J8_30", "requests": N_STREAM,
              "requests_per_step": REQ_PER_STEP, "atoms": int(atoms_total),
@@ -819,6 +824,9 @@ def run_batch512(args, torch, lds, dev, world, rank, local, dist):
     st = eng.serve(reqs, None)
     serve_s = time.perf_counter() - t0
     eng.close()
+    # whole-job rates: all ranks' atoms over the slowest rank's time
+    e2e_rate, _, _ = replica_throughput(n_rows, 1e3 * e2e_s, dist, dev)
+    serve_rate, _, _ = replica_throughput(n_rows, 1e3 * serve_s, dist, dev)
     if rank != 0:
         return None
     flop = {k: sum(algorithmic_flops(specs[k], c, weights) for c in cfgs) for k in specs}
@@ -865,12 +873,12 @@ def run_batch512(args, torch, lds, dev, world, rank, local, dist):
         "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded cells, no dataset)", "config": cdesc,
         "roofline": roof, "cpu_baseline": cpu, "parity": parity,
-        "e2e": {"value": world * n_rows / e2e_s, "unit": "atoms/s", "h2d_bytes_per_step": int(h2d),
+        "e2e": {"value": e2e_rate, "unit": "atoms/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * e2e_s,
                 "api": "batch.DeviceBatch.from_batch once (pinned host batch) + BatchedPass.run per descriptor, "
                        "dE up and descriptors and forces back to pinned host memory on a copy stream that "
                        "overlaps the passes, synchronised, every step",
-                "serving_engine": {"value": world * n_rows / serve_s, "ms_per_step": 1e3 * serve_s,
+                "serving_engine": {"value": serve_rate, "ms_per_step": 1e3 * serve_s,
                                    "api": "ServingEngine.serve of the 1024 (cell, descriptor) requests, host numpy "
                                           "in/out", "batches": st["batches"]}},
         "gpu_launches": int(launches), "clocks": clk.summary([(t_a, t_b)]),
@@ -949,9 +957,10 @@ def run_single(args, torch, lds, dev, world, rank, local, dist):
     for _ in range(ke):
         lds.compute_and_gradient(ds, n, h_sp, h_nbl, h_cnt, h_x, h_dE)
     e2e_s = (time.perf_counter() - t0) / ke
+    e2e_rate, _, _ = replica_throughput(n, 1e3 * e2e_s, dist, dev)
     h2d = cfg.species.nbytes + cfg.nbl.nbytes + cfg.counts.nbytes + cfg.coords.nbytes + dE_h.nbytes + 8 * (n + 1)
     d2h = 8 * n * W + 8 * 3 * cfg.n_total
-    e2e = {"value": world * n / e2e_s, "unit": "atoms/s", "h2d_bytes_per_step": int(h2d),
+    e2e = {"value": e2e_rate, "unit": "atoms/s", "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * e2e_s,
            "api": "libdescriptor_b200.compute_and_gradient (numpy inputs in pinned host memory, numpy results out, one fused pass)"}
     if rank != 0:
