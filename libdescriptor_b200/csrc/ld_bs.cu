@@ -100,15 +100,15 @@ __device__ __forceinline__ double sfac_of(const BSDev &p, double r, double rc) {
     if (p.switch_flag == 1) {
         if (r <= p.rmin0) return 1.0;
         if (r > rc) return 0.0;
-        return 0.5 * (cos((r - p.rmin0) * kPi / (rc - p.rmin0)) + 1.0);
+        return 0.5 * (cospi((r - p.rmin0) / (rc - p.rmin0)) + 1.0);
     }
     return 0.0;
 }
 __device__ __forceinline__ double dsfac_of(const BSDev &p, double r, double rc) {
     if (p.switch_flag == 1) {
         if (r <= p.rmin0 || r > rc) return 0.0;
-        const double f = kPi / (rc - p.rmin0);
-        return -0.5 * sin((r - p.rmin0) * f) * f;
+        const double inv = 1.0 / (rc - p.rmin0);
+        return -0.5 * sinpi((r - p.rmin0) * inv) * (kPi * inv);
     }
     return 0.0;
 }
@@ -216,9 +216,11 @@ __global__ void __launch_bounds__(NT) bs_kernel(BSDev p, RowArgs a, int cap) {
                 const double rsq = x * x + y * y + z * z;
                 const double r = sqrt(rsq);
                 const double rc = C.src[k];
-                const double theta0 = (r - p.rmin0) * p.rfac0 * kPi / (rc - p.rmin0);
-                const double z0 = r / tan(theta0);
-                const double r0inv = 1.0 / sqrt(r * r + z0 * z0);
+                // z0 = r / tan(theta0) from one sincos and one reciprocal
+                double sth, cth;
+                sincos((r - p.rmin0) * (p.rfac0 * kPi / (rc - p.rmin0)), &sth, &cth);
+                const double z0 = r * cth / sth;
+                const double r0inv = rsqrt(r * r + z0 * z0);
                 const double a_r = r0inv * z0, a_i = -r0inv * z;
                 const double b_r = r0inv * y, b_i = -r0inv * x;
                 const double sf = sfac_of(p, r, rc) * C.sw[k];
@@ -428,12 +430,12 @@ __global__ void __launch_bounds__(NT) bs_kernel(BSDev p, RowArgs a, int cap) {
                 const double r = sqrt(rsq);
                 const double rc = C.src[k];
                 const double c0 = p.rfac0 * kPi / (rc - p.rmin0);
-                const double theta0 = (r - p.rmin0) * p.rfac0 * kPi / (rc - p.rmin0);
                 double sth, cth;
-                sincos(theta0, &sth, &cth);
-                const double z0 = r / tan(theta0);
-                const double dz0 = cth / sth - r * c0 / (sth * sth);
-                const double r0inv = 1.0 / sqrt(r * r + z0 * z0);
+                sincos((r - p.rmin0) * c0, &sth, &cth);
+                const double isth = 1.0 / sth;
+                const double z0 = r * cth * isth;
+                const double dz0 = cth * isth - r * c0 * isth * isth;
+                const double r0inv = rsqrt(r * r + z0 * z0);
                 const double dr0inv = -r0inv * r0inv * r0inv * (r + z0 * dz0);
                 const double a_r = r0inv * z0, a_i = -r0inv * z;
                 const double b_r = r0inv * y, b_i = -r0inv * x;
