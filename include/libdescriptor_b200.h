@@ -416,6 +416,14 @@ int ld_fail_next_allocation(int k);
  * off.  Costs one memset per allocation while on. */
 int ld_debug_fill_scratch(int byte);
 
+/* Self-test of the kernels' bounded waits (no reference counterpart): one
+ * CTA arms a shared-memory barrier for a bulk copy that is never issued and
+ * waits for it at most limit_ns nanoseconds of device time (1 .. 1e9), the
+ * same wait the Z kernel uses for its bulk-copied U tile.  Returns
+ * LD_ERR_TIMEOUT when the wait ran out -- the expected outcome -- with the
+ * device left usable; LD_OK would mean the wait never gave up. */
+int ld_debug_bulk_wait_timeout(long long limit_ns);
+
 /* Pinned (page-locked) host memory for results: the device writes into it at
  * the link's rate, where a copy into fresh pageable memory runs several
  * times slower.  Blocks are rounded up to 64 KiB; a released block is kept

@@ -40,7 +40,7 @@ CORE_SOURCES = ["ld_sf.cu", "ld_bs.cu", "ld_util.cu", "ld_core.cpp", "ld_neighbo
                 "ld_bs2_j10.cu", "ld_serve.cpp", "ld_sfg.cu", "ld_neighbor_dev.cu", "ld_sfp.cu"]
 # host threads for the serving runtime's request staging
 EXTRA_FLAGS = {"ld_serve.cpp": ["-Xcompiler", "-fopenmp"]}
-HEADERS = [os.path.join(CSRC, "ld_internal.h"), os.path.join(CSRC, "ld_neighbor_math.h"), os.path.join(CSRC, "ld_sf_common.cuh"), os.path.join(CSRC, "ld_csr.cuh"), os.path.join(CSRC, "ld_bs2.cuh"),
+HEADERS = [os.path.join(CSRC, "ld_internal.h"), os.path.join(CSRC, "ld_neighbor_math.h"), os.path.join(CSRC, "ld_sf_common.cuh"), os.path.join(CSRC, "ld_csr.cuh"), os.path.join(CSRC, "ld_bulk.cuh"), os.path.join(CSRC, "ld_bs2.cuh"),
            os.path.join(CSRC, "ld_bs2_impl.cuh"), os.path.join(INCLUDE, "libdescriptor_b200.h")]
 
 

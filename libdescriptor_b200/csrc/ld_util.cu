@@ -2,6 +2,7 @@
 #include <cub/cub.cuh>
 #include <mutex>
 
+#include "ld_bulk.cuh"
 #include "ld_internal.h"
 
 namespace ldb {
@@ -126,7 +127,44 @@ int offsets_launch(int n_rows, const int *counts, long long *off, int *maxn, voi
     return LD_OK;
 }
 
+// Self-test of the bounded bulk-copy wait: thread 0 arms the barrier for 16
+// bytes that no copy delivers, every thread waits at most limit_ns, and the
+// CTA reports kDevTimeout when the wait ran out (it always should).
+__global__ void bulk_wait_probe(unsigned long long limit_ns, int *status) {
+    __shared__ __align__(8) unsigned long long bar;
+    if (threadIdx.x == 0) {
+        bulk_barrier_init(&bar);
+        bulk_expect(&bar, 16);
+    }
+    __syncthreads();
+    const bool ok = bulk_copy_wait(&bar, limit_ns);
+    if (__syncthreads_or(!ok) && threadIdx.x == 0) atomicCAS(status, 0, (int)kDevTimeout);
+}
+
 }  // namespace ldb
+
+extern "C" int ld_debug_bulk_wait_timeout(long long limit_ns) {
+    using namespace ldb;
+    if (limit_ns <= 0 || limit_ns > 1000000000LL)
+        return fail(LD_ERR_INVALID_ARG, "ld_debug_bulk_wait_timeout: limit_ns outside 1 .. 1e9");
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return fail(LD_ERR_NO_DEVICE, "no CUDA device visible");
+    int *status = nullptr;
+    LDB_CUDA(cudaMalloc(&status, sizeof(int)));
+    int host = -1;
+    cudaError_t e = cudaMemset(status, 0, sizeof(int));
+    if (e == cudaSuccess) {
+        bulk_wait_probe<<<1, 64>>>((unsigned long long)limit_ns, status);
+        count_launch();
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(&host, status, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(status);
+    if (e != cudaSuccess) return cuda_fail(e, "bulk_wait_probe");
+    if (host == kDevTimeout)
+        return fail(LD_ERR_TIMEOUT, "ld_debug_bulk_wait_timeout: the bounded wait ran out (as it should)");
+    return LD_OK;
+}
 
 extern "C" int ld_measure_fp64_peak(int iters, double *tflops) {
     using namespace ldb;

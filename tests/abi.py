@@ -52,6 +52,7 @@ class Abi:
             L.ld_alloc_count.restype = C.c_longlong
             L.ld_fail_next_allocation.argtypes = [C.c_int]
             L.ld_debug_fill_scratch.argtypes = [C.c_int]
+            L.ld_debug_bulk_wait_timeout.argtypes = [C.c_longlong]
             L.ld_create_symmetry_functions.argtypes = [C.POINTER(C.c_void_p), C.c_int, _dp, C.c_int,
                                                        _ip, _ip, _dp]
             L.ld_create_bispectrum.argtypes = [C.POINTER(C.c_void_p), C.c_double, C.c_int, C.c_int,

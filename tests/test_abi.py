@@ -142,3 +142,15 @@ def test_scratch_fill_hook_checks_its_byte():
     assert L.ld_debug_fill_scratch(256) == 2
     assert L.ld_debug_fill_scratch(0xFF) == 0
     assert L.ld_debug_fill_scratch(-1) == 0
+
+
+def test_bulk_wait_self_test_checks_its_limit():
+    """ld_debug_bulk_wait_timeout takes 1 .. 1e9 ns and needs a device (the
+    GPU test makes the wait run out)."""
+    import torch
+
+    L = Abi.lib()
+    assert L.ld_debug_bulk_wait_timeout(0) == 2
+    assert L.ld_debug_bulk_wait_timeout(2 * 10**9) == 2
+    if not torch.cuda.is_available():
+        assert L.ld_debug_bulk_wait_timeout(1000) == 7          # LD_ERR_NO_DEVICE

@@ -9,6 +9,8 @@
 * Cancellation: requests withdrawn from the serving engine while they wait
   (pending or admitted, not launched) get no results and free their ring
   space; every other request's results are those it gets alone.
+* Bounded waits: a bulk-copy wait armed for a copy that never comes gives up
+  after its limit and reports LD_ERR_TIMEOUT; the device stays usable.
 """
 import numpy as np
 import pytest
@@ -133,3 +135,21 @@ def test_cancelled_requests_leave_the_rest_unchanged():
         assert_close(r.grad, gr, GRAD_RTOL, f"request {r.rid} forces")
     for rings in eng.sched.rings.values():
         assert all(ring.used == 0 for ring in rings)
+
+
+def test_bounded_bulk_wait_runs_out_and_device_stays_usable():
+    """The Z kernel's wait for its bulk-copied tile is bounded: armed for a
+    copy that never comes, the same wait gives up after its limit and the CTA
+    reports a timeout (LD_ERR_TIMEOUT) instead of hanging; the device then
+    computes the reference's results as before."""
+    import time
+
+    L = Abi.lib()
+    t0 = time.perf_counter()
+    assert L.ld_debug_bulk_wait_timeout(2_000_000) == 6      # LD_ERR_TIMEOUT after ~2 ms of device time
+    assert time.perf_counter() - t0 < 30.0
+    assert "ran out" in L.ld_error_message().decode()
+    g = load_golden("bs_j8_style3_sw1_packing64")
+    h = gpu_for("bs_j8_style3_sw1_packing64", g)
+    desc = h.compute(int(g["n_atoms"]), g["species"], g["nbl"], g["counts"], g["coords"])
+    assert_close(desc, g["desc"], DESC_RTOL, "descriptors after the timed-out wait")
