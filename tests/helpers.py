@@ -1,7 +1,7 @@
 """Test helpers: build the oracle and the GPU descriptor for a golden fixture,
 and the tolerance rule used by every parity test.
 
-Tolerance (descriptors 1e-10 relative, gradients 1e-8):
+Tolerance (the parity bar: descriptors 1e-10 relative, gradients 1e-8):
 an element passes when
 
     |x - ref| <= rtol * max(|ref|, 1e-3 * scale_c)
