@@ -125,7 +125,7 @@ def fd_pin(ref, x, s, counts, nbl, width, centres, seed):
 def main():
     oracle.build(with_ref=True)
     rc = 5.0
-    # C1: 64-atom diamond, SF 24
+    # the 64-atom diamond with the 24-d symmetry functions
     x, cell = diamond(2, jitter=0.05, seed=0)
     sp = np.zeros(len(x), np.int32)
     allx, alls, counts, nbl, image = layout(x, cell, sp, rc)
