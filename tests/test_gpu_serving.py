@@ -94,3 +94,35 @@ def test_style2_bispectrum_lane_with_nan_filled_work_space():
     eng.serve(reqs, None, keep_results=True)
     eng.close()
     _check(reqs, alone)
+
+
+def test_requests_without_neighbours_in_the_mix(stream_setup):
+    """Requests whose atoms have no neighbours at all (an empty neighbour
+    field in their staging chunk) between ordinary ones: every result equals
+    its plain call (isolated atoms: zero forces, the descriptors of an empty
+    environment)."""
+    import libdescriptor_b200 as lds
+    from libdescriptor_b200 import serving as S
+
+    kinds, pool, widths, _ = stream_setup
+    reqs = S.make_requests(pool, 12, widths, {"sf": 0.5, "bs": 0.5}, seed=21)
+    rng = np.random.default_rng(22)
+    mixed = []
+    for i, r in enumerate(reqs):
+        mixed.append(r)
+        n = 1 + i % 3
+        lane = "sf" if i % 2 else "bs"
+        coords = rng.normal(size=(n, 3)) * 20.0          # far apart: no neighbours within 5 A
+        mixed.append(S.Request(1000 + i, lane, n, coords, np.zeros(n, np.int32), np.arange(n, dtype=np.int32),
+                               np.zeros(n, np.int32), np.zeros(0, np.int32),
+                               rng.normal(size=(n, widths[lane]))))
+    for k, r in enumerate(mixed):
+        r.rid = k
+    alone = []
+    for r in mixed:
+        d, g = lds.compute_and_gradient(kinds[r.lane], r.n_atoms, r.species, r.nbl, r.counts, r.coords, r.dE)
+        alone.append((d, S.fold_host(g, r.n_atoms, r.image)))
+    eng = S.ServingEngine(kinds, budget_bytes=64 << 20, max_batch_rows=2048, stage_bytes=8 << 20)
+    eng.serve(mixed, None, keep_results=True)
+    eng.close()
+    _check(mixed, alone)
