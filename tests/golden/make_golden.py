@@ -162,6 +162,13 @@ def main():
         save(f"bs_j{J}_style{style}_sw{sw}_packing64", n_atoms=64, coords=allx, species=alls,
              counts=counts, nbl=nbl, image=image, cutoff=rc, twojmax=J, style=style,
              switch_flag=sw, rfac0=0.99363, rmin0=0.0, weights=np.array([1.0, 0.5]), desc=desc, **kw)
+    # bzero_flag: the reference subtracts bzero[j] = j w_self^3 from every
+    # B of output layer j (src/Bispectrum.cpp:64-67, 423)
+    ref = ReferenceDescriptor.bispectrum(0.99363, 6, 3, 0.0, 1, 1, 2, cm, [1.0, 0.5])
+    desc = ref.compute(64, alls, nbl, counts, allx)
+    save("bs_j6_bzero_packing64", n_atoms=64, coords=allx, species=alls, counts=counts, nbl=nbl,
+         image=image, cutoff=rc, twojmax=6, style=3, switch_flag=1, bzero_flag=1, rfac0=0.99363, rmin0=0.0,
+         weights=np.array([1.0, 0.5]), desc=desc)
     # non-uniform species-pair cutoffs: the reference reads the bispectrum
     # cutoff as element [jSpecies] of the flattened matrix
     cmq = np.array([[5.0, 4.0], [4.5, 3.5]])

@@ -59,6 +59,11 @@ def n_species_of(g):
     return int(np.max(g["species"])) + 1
 
 
+def bzero_of(g) -> int:
+    """The golden's bzero_flag (fixtures made before it was recorded: 0)."""
+    return int(g["bzero_flag"]) if "bzero_flag" in g else 0
+
+
 def oracle_for(name, g):
     from oracle import OracleDescriptor
 
@@ -67,7 +72,7 @@ def oracle_for(name, g):
         t, s, p = sf_params_of(name)
         return OracleDescriptor.symmetry_functions(ns, cutoff_matrix(g, ns), t, s, p)
     return OracleDescriptor.bispectrum(float(g["rfac0"]), int(g["twojmax"]), int(g["style"]),
-                                       float(g["rmin0"]), int(g["switch_flag"]), 0, ns,
+                                       float(g["rmin0"]), int(g["switch_flag"]), bzero_of(g), ns,
                                        cutoff_matrix(g, ns), g["weights"])
 
 
@@ -80,4 +85,4 @@ def gpu_for(name, g):
         t, s, p = sf_params_of(name)
         return Abi.create_sf(ns, cutoff_matrix(g, ns), t, s, p)
     return Abi.create_bs(float(g["rfac0"]), int(g["twojmax"]), int(g["style"]), float(g["rmin0"]),
-                         int(g["switch_flag"]), 0, ns, cutoff_matrix(g, ns), g["weights"])
+                         int(g["switch_flag"]), bzero_of(g), ns, cutoff_matrix(g, ns), g["weights"])
