@@ -59,16 +59,17 @@ __device__ __forceinline__ double sfac_of(const BSDev &p, double r, double rc) {
     }
     return 0.0;
 }
-// the switching function and its derivative together (one division, one
-// sincospi of (r - rmin0) / (rc - rmin0))
-__device__ __forceinline__ void sfac_both(const BSDev &p, double r, double rc, double &sf, double &dsf) {
+// the switching function and its derivative together (one sincospi of
+// (r - rmin0) * isw, isw = 1 / (rc - rmin0) from the per-species table)
+__device__ __forceinline__ void sfac_both(const BSDev &p, double r, double rc, double isw, double &sf,
+                                          double &dsf) {
     sf = p.switch_flag == 0 ? 1.0 : 0.0;
     dsf = 0.0;
     if (p.switch_flag == 1) {
         if (r <= p.rmin0) {
             sf = 1.0;
         } else if (!(r > rc)) {
-            const double inv = 1.0 / (rc - p.rmin0);
+            const double inv = isw;
             double sn, cs;
             sincospi((r - p.rmin0) * inv, &sn, &cs);
             sf = 0.5 * (cs + 1.0);
@@ -92,13 +93,13 @@ struct CK {
     double dar[3], dai[3], dbr[3], dbi[3];
 };
 
+// with c0 = rfac0 pi / (rc - rmin0) given (the per-species table ang_flat)
 template <bool TAN>
-__device__ __forceinline__ void cayley_klein(const BSDev &p, double x, double y, double z, double r, double rc,
-                                             CK &c) {
+__device__ __forceinline__ void cayley_klein_c0(double rmin0, double x, double y, double z, double r, double c0,
+                                                CK &c) {
     // theta0 = (r - rmin0) c0, z0 = r / tan(theta0) = r cos / sin: one
     // sincos and one reciprocal serve the parameters and their tangents
-    const double c0 = p.rfac0 * kPi / (rc - p.rmin0);
-    const double theta0 = (r - p.rmin0) * c0;
+    const double theta0 = (r - rmin0) * c0;
     double sth, cth;
     sincos(theta0, &sth, &cth);
     const double isth = 1.0 / sth;
@@ -121,6 +122,12 @@ __device__ __forceinline__ void cayley_klein(const BSDev &p, double x, double y,
             c.dbi[d] = -(x * dr0inv * u3[d] + (d == 0 ? r0inv : 0.0));
         }
     }
+}
+
+template <bool TAN>
+__device__ __forceinline__ void cayley_klein(const BSDev &p, double x, double y, double z, double r, double rc,
+                                             CK &c) {
+    cayley_klein_c0<TAN>(p.rmin0, x, y, z, r, p.rfac0 * kPi / (rc - p.rmin0), c);
 }
 
 // One layer j of the column recursion for this lane's column mb (in place).

@@ -761,6 +761,14 @@ static int build_bs_impl(ld_descriptor *d, double rfac0, int J, int style, doubl
     for (auto &t : trip) trip4.push_back(make_int4(t[0], t[1], t[2], t[3]));
     Arena ar;
     ar.add(rcut_flat, &b.rcut_flat);
+    std::vector<double> ang_flat(ns), isw_flat(ns);
+    for (int k = 0; k < ns; ++k) {
+        const double span = rcut_flat[k] - rmin0;
+        ang_flat[k] = span > 0.0 ? rfac0 * 3.1415926535897932 / span : 0.0;
+        isw_flat[k] = span > 0.0 ? 1.0 / span : 0.0;
+    }
+    ar.add(ang_flat, &b.ang_flat);
+    ar.add(isw_flat, &b.isw_flat);
     ar.add(wj, &b.wj);
     ar.add(bzero, &b.bzero);
     ar.add(rootpq, &b.rootpq);

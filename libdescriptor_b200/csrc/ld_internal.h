@@ -125,6 +125,8 @@ struct BSDev {
     int ncoeff = 0, nU = 0, nL = 0, ntrip = 0, nZall = 0, ncg = 0;
     double rfac0 = 0, rmin0 = 0, wself = 1.0;
     const double *rcut_flat = nullptr;  // per neighbour species (reference quirk)
+    const double *ang_flat = nullptr;   // per neighbour species: rfac0 pi / (rc - rmin0)
+    const double *isw_flat = nullptr;   // per neighbour species: 1 / (rc - rmin0)
     const double *wj = nullptr;         // per species weight
     const double *bzero = nullptr;      // J+1
     const double *rootpq = nullptr;     // (J+1)^2, [p*(J+1)+q] = sqrt(p/q)

@@ -146,7 +146,7 @@ sf_kernel(SFDev p, RowArgs a, int per_warp_doubles, int *queue) {
                     }
                 }
                 if (VJP) {
-                    const double inv = 1.0 / r;
+                    const double inv = S.ir[jj];
                     const double gx = dsum * (S.cx[jj] - cix) * inv;
                     const double gy = dsum * (S.cy[jj] - ciy) * inv;
                     const double gz = dsum * (S.cz[jj] - ciz) * inv;

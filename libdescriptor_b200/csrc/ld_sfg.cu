@@ -175,7 +175,7 @@ sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue)
                     }
                 }
                 if (VJP) {
-                    const double inv = 1.0 / r;
+                    const double inv = S.ir[jj];
                     const double gx = dsum * (S.cx[jj] - cix) * inv;
                     const double gy = dsum * (S.cy[jj] - ciy) * inv;
                     const double gz = dsum * (S.cz[jj] - ciz) * inv;
