@@ -231,10 +231,6 @@ struct RowArgs {
 #ifndef LD_ZTILE_B
 #define LD_ZTILE_B 2
 #endif
-// 1: the Clebsch-Gordan table is copied to each CTA's shared memory
-#ifndef LD_CG_SHARED
-#define LD_CG_SHARED 1
-#endif
 constexpr int kZTileA = LD_ZTILE_A;
 constexpr int kZTileB = LD_ZTILE_B;
 

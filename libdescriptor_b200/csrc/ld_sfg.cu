@@ -21,15 +21,12 @@ namespace {
 using namespace sfc;
 
 constexpr int NA = kSFGA, NR = kSFGR;
-// 1: the row's gP(a, r) = dL/dG * 2^(1-zeta) live in the warp's shared slice
-// (warp-uniform reads) instead of registers
-#ifndef LD_SFG_GP_SHARED
-#define LD_SFG_GP_SHARED 1
-#endif
 #ifndef LD_SFG_MINB
 #define LD_SFG_MINB 4
 #endif
-constexpr int kGPExtra = (LD_SFG_GP_SHARED ? 2 * NA * NR : 0);
+// the row's gP(a, r) = dL/dG * 2^(1-zeta) live at the end of the warp's
+// shared slice (warp-uniform reads) instead of in registers
+constexpr int kGPExtra = 2 * NA * NR;
 // radial terms of a triplet: E0 = exp(-eta_0 S) once, its squarings
 // E0^(2^k) once, and each integer multiple eta_r = k eta_0 (k < 2^kSFGPowBits)
 // as a balanced product of the squarings its bits select: a dependent chain
@@ -199,11 +196,7 @@ sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue)
         if (PH != 2 && (HAS4 || HAS5)) {
             constexpr int NT = 2;
             double acc[NT][NA][NR];
-#if LD_SFG_GP_SHARED
             double(*gP)[NA][NR] = reinterpret_cast<double(*)[NA][NR]>(smem + (size_t)warp * per_warp + per_warp - kGPExtra);
-#else
-            double gP[NT][NA][NR];
-#endif
 #pragma unroll
             for (int ty = 0; ty < NT; ++ty)
 #pragma unroll
@@ -214,16 +207,10 @@ sfg_kernel(const __grid_constant__ SFDev p, RowArgs a, int per_warp, int *queue)
                         acc[ty][x][y] = 0.0;
                         double v = 0.0;
                         if (VJP && on && g.out[ty][x][y] >= 0) v = __ldg(dE + g.out[ty][x][y]) * g.P[ty][x];
-#if LD_SFG_GP_SHARED
                         // the slice has room for gP only in the gradient kernel
                         if (VJP && lane == 0) gP[ty][x][y] = v;
-#else
-                        gP[ty][x][y] = v;
-#endif
                     }
-#if LD_SFG_GP_SHARED
             if (VJP) __syncwarp();
-#endif
             // Lane l owns neighbours jj = l, l + 32, ...; at step dd it takes the
             // triplet (jj, kk = (jj + dd) mod n), dd = 1 .. n/2 (the last step,
             // for even n, only for jj < n/2): every unordered pair once, and
