@@ -627,18 +627,25 @@ class ServingEngine:
             for req, off in zip(reqs, offsets):
                 jobs.append((req, [blk + st + o for st, o in zip(starts, off)]))
             total += nbytes
-        if self._pool is None or len(jobs) == 1 or total < (4 << 20):
-            self._pack_group(jobs)
-        else:
-            # longest first onto the least loaded of the workers
-            groups = [[] for _ in range(min(self._pack_threads, len(jobs)))]
-            load = [0] * len(groups)
-            for job in sorted(jobs, key=lambda j: -(j[0].n_total + j[0].nnz + j[0].n_atoms * ln.W)):
-                g = load.index(min(load))
-                groups[g].append(job)
-                load[g] += job[0].n_total + job[0].nnz + job[0].n_atoms * ln.W
-            for f in [self._pool.submit(self._pack_group, g) for g in groups]:
-                f.result()
+        try:
+            if self._pool is None or len(jobs) == 1 or total < (4 << 20):
+                self._pack_group(jobs)
+            else:
+                # longest first onto the least loaded of the workers
+                groups = [[] for _ in range(min(self._pack_threads, len(jobs)))]
+                load = [0] * len(groups)
+                for job in sorted(jobs, key=lambda j: -(j[0].n_total + j[0].nnz + j[0].n_atoms * ln.W)):
+                    g = load.index(min(load))
+                    groups[g].append(job)
+                    load[g] += job[0].n_total + job[0].nnz + job[0].n_atoms * ln.W
+                for f in [self._pool.submit(self._pack_group, g) for g in groups]:
+                    f.result()
+        except Exception:
+            # a request failed its index checks: give the chunks' staging
+            # blocks back before the error reaches the caller
+            for _, u0, _ in chunks:
+                ln.stage_ring.release(u0)
+            raise
         W = ln.W
         for reqs, u0, (starts, totals, offsets, nbytes) in chunks:
             r0, a0, e0 = reqs[0].slots

@@ -126,3 +126,22 @@ def test_requests_without_neighbours_in_the_mix(stream_setup):
     eng.serve(mixed, None, keep_results=True)
     eng.close()
     _check(mixed, alone)
+
+
+def test_request_with_bad_index_raises_and_frees_staging(stream_setup):
+    """A request whose neighbour list points outside its atoms fails its
+    host-side index check during staging: ``serve`` raises, and the staging
+    blocks reserved for that round are given back."""
+    from libdescriptor_b200 import serving as S
+
+    kinds, pool, widths, _ = stream_setup
+    reqs = S.make_requests(pool, 3, widths, {"sf": 1.0}, seed=31)
+    bad = reqs[1]
+    nbl = np.array(bad.nbl, copy=True)
+    nbl[0] = bad.n_total + 5
+    reqs[1] = S.Request(bad.rid, bad.lane, bad.n_atoms, bad.coords, bad.species, bad.image, bad.counts, nbl, bad.dE)
+    eng = S.ServingEngine(kinds, budget_bytes=64 << 20, max_batch_rows=2048, stage_bytes=8 << 20)
+    with pytest.raises((ValueError, RuntimeError), match="outside"):
+        eng.serve(reqs, None)
+    assert all(ln.stage_ring.used == 0 for ln in eng.lanes.values())
+    eng.close()
