@@ -4,8 +4,8 @@
 // bytes); the other threads do independent set-up meanwhile and then wait
 // for the barrier's phase 0.  The wait is bounded in time (the device's
 // nanosecond timer) and in rounds: past either limit it returns false and
-// the caller reports kDevTimeout instead of spinning.  Local memory only (no
-// multicast, no peer memory).
+// the caller reports kDevTimeout instead of spinning.  Every copy is the
+// CTA's own, from this GPU's own memory.
 #pragma once
 
 namespace ldb {
